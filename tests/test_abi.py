@@ -1,0 +1,60 @@
+"""The C ABI library loads and exports every function include/cp_prover.h declares."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", fn)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_\s\*]*?\b(cp_[A-Za-z0-9_]+)\s*\(", text, re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+@pytest.fixture(scope="module")
+def libpath():
+    from circlepacking_b200 import build
+
+    return build.build()
+
+
+def test_header_declares_functions():
+    names = declared_functions()
+    assert "cp_eval_boxes" in names and "cp_lattice_boxes" in names
+
+
+def test_library_exports_all_declared(libpath):
+    out = subprocess.run(["nm", "-D", "--defined-only", libpath], capture_output=True, text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = [n for n in declared_functions() if n not in exported]
+    assert not missing, missing
+
+
+def test_library_loads_and_reports(libpath):
+    import circlepacking_b200 as cp
+
+    L = cp.lib()
+    assert L.cp_family_dims(3) == 4 and L.cp_family_dims(1) == 3 and L.cp_family_dims(9) == -1
+    assert L.cp_family_criteria(3) == 4
+    assert L.cp_status_string(0) == b"ok"
+    assert b"sm_100a" in L.cp_version()
+
+
+def test_invalid_arguments_rejected_without_device(libpath):
+    import circlepacking_b200 as cp
+
+    L = cp.lib()
+    # argument validation happens before any CUDA call
+    assert L.cp_eval_boxes(7, 0, 0, None, None, 10, 10, None, None, None, None, None) == 1
+    assert L.cp_eval_boxes(3, 5, 0, None, None, 10, 10, None, None, None, None, None) == 1
+    assert L.cp_eval_boxes(3, 0, 0, None, None, 0, 0, None, None, None, None, None) == 0
