@@ -70,7 +70,7 @@ def _declare(L):
     L.cp_version.restype = ctypes.c_char_p
     L.cp_eval_boxes.argtypes = [I, I, I, P, P, SZ, SZ, P, P, P, P, P]
     L.cp_eval_boxes_host.argtypes = [I, I, I, P, P, SZ, P, P]
-    L.cp_lattice_boxes.argtypes = [I, D, D, P, P, SZ, P, P, SZ, P]
+    L.cp_lattice_boxes.argtypes = [I, D, D, P, P, SZ, P, P, SZ, P, P]
     L.cp_single_placement.argtypes = [P, SZ, P, P]
     L.cp_eval_primitive.argtypes = [I, P, SZ, P, P, P]
     L.cp_asin_pad.argtypes = [P, SZ, P, P, P]
@@ -135,8 +135,9 @@ def eval_boxes_host(family: int, lo: np.ndarray, hi: np.ndarray, precision: int 
     return v, m
 
 
-def lattice_boxes(family: int, outer, sizes, index):
-    """Raw boxes of a family lattice at the given linear indices (CUDA tensors (dims, n))."""
+def lattice_boxes(family: int, outer, sizes, index, visited: bool = False):
+    """Raw boxes of a family lattice at the given linear indices (CUDA tensors
+    (dims, n)); with visited=True also the byte mask of boxes the kernel visits."""
     torch = _torch()
     idx = _dev(index, torch.int64)
     n = idx.numel()
@@ -144,9 +145,10 @@ def lattice_boxes(family: int, outer, sizes, index):
     s = (ctypes.c_int32 * 4)(*(list(sizes) + [1] * (4 - len(sizes))))
     lo = torch.empty((dims, n), dtype=torch.float64, device="cuda")
     hi = torch.empty((dims, n), dtype=torch.float64, device="cuda")
+    vis = torch.empty(n, dtype=torch.uint8, device="cuda") if visited else None
     _check(lib().cp_lattice_boxes(family, float(outer[0]), float(outer[1]), s, _ptr(idx), n, _ptr(lo), _ptr(hi), n,
-                                  _stream()), "cp_lattice_boxes")
-    return lo, hi
+                                  _ptr(vis), _stream()), "cp_lattice_boxes")
+    return (lo, hi, vis) if visited else (lo, hi)
 
 
 def single_placement(lb_lambda):
@@ -177,3 +179,188 @@ def asin_pad(x):
     ru = torch.empty_like(x)
     _check(lib().cp_asin_pad(_ptr(x), x.numel(), _ptr(rd), _ptr(ru), _stream()), "cp_asin_pad")
     return rd, ru
+
+
+# ---------------------------------------------------------------- prover handle
+SPLIT_UNIFORM, SPLIT_LAMBDA, SPLIT_WIDEST, SPLIT_LEARNED = range(4)
+REFERENCE_SIZES = ((256, 256, 256, 64), (4096, 4096, 4096), (256, 256, 256, 64), (512, 256, 256, 64),
+                   (4096, 1024, 1024), (1024, 256, 128, 128))
+
+
+class RefineOpts(ctypes.Structure):
+    _fields_ = [("family", ctypes.c_int32), ("precision", ctypes.c_int32), ("policy", ctypes.c_int32),
+                ("max_depth", ctypes.c_int32), ("seed_sizes", ctypes.c_int32 * 4), ("seed_lambda", ctypes.c_double * 2),
+                ("level_capacity", ctypes.c_int64), ("block", ctypes.c_int32), ("learned_order", ctypes.c_int32)]
+
+
+class RefineReport(ctypes.Structure):
+    _fields_ = [("evaluated", ctypes.c_int64), ("verdicts", ctypes.c_int64 * 5), ("unresolved", ctypes.c_int64),
+                ("clipped", ctypes.c_int64), ("fp32_decided", ctypes.c_int64), ("per_depth", ctypes.c_int64 * 64),
+                ("max_depth_seen", ctypes.c_int32), ("launches", ctypes.c_int32), ("device_ms", ctypes.c_double),
+                ("wall_ms", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return dict(evaluated=self.evaluated, verdicts=list(self.verdicts), unresolved=self.unresolved,
+                    clipped=self.clipped, fp32_decided=self.fp32_decided,
+                    per_depth=list(self.per_depth)[: self.max_depth_seen + 1], launches=self.launches,
+                    device_ms=self.device_ms, wall_ms=self.wall_ms)
+
+
+class ReferenceReport(ctypes.Structure):
+    _fields_ = [("proved", ctypes.c_int32), ("interrupted", ctypes.c_int32), ("launches", ctypes.c_int64),
+                ("boxes_evaluated", ctypes.c_int64), ("remaining", ctypes.c_double * 2), ("device_ms", ctypes.c_double),
+                ("wall_ms", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return dict(proved=bool(self.proved), interrupted=bool(self.interrupted), launches=self.launches,
+                    boxes_evaluated=self.boxes_evaluated, remaining=list(self.remaining), device_ms=self.device_ms,
+                    wall_ms=self.wall_ms)
+
+
+def _declare_handle(L):
+    P, I, D, SZ, I64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t, ctypes.c_int64
+    L.cp_create.argtypes = [I, ctypes.POINTER(P)]
+    L.cp_destroy.argtypes = [P]
+    L.cp_destroy.restype = None
+    L.cp_request_interrupt.argtypes = [P]
+    L.cp_request_interrupt.restype = None
+    L.cp_refine.argtypes = [P, ctypes.POINTER(RefineOpts), ctypes.POINTER(RefineReport)]
+    L.cp_refine_boxes.argtypes = [P, ctypes.POINTER(RefineOpts), P, P, P, SZ, ctypes.POINTER(RefineReport)]
+    L.cp_refine_boxes_host.argtypes = [P, ctypes.POINTER(RefineOpts), P, P, P, SZ, ctypes.POINTER(RefineReport)]
+    L.cp_reference_step.argtypes = [P, I, D, D, P, P, P]
+    L.cp_prove_family_reference.argtypes = [P, I, D, D, P, I64, P, ctypes.POINTER(ReferenceReport)]
+    L.cp_reference_criticals.argtypes = [P, I, D, D, P, SZ, P, P, ctypes.POINTER(SZ)]
+    L.cp_measure_primitives.argtypes = [I, P]
+    L.cp_get_stream.argtypes = [P]
+    L.cp_get_stream.restype = P
+    L.cp_autotune.argtypes = [P, ctypes.POINTER(RefineOpts), ctypes.POINTER(ctypes.c_int), P]
+    L.cp_set_level_variant.argtypes = [P, I, I, I]
+
+
+def measure_primitives(device: int = 0) -> dict:
+    L = lib()
+    _declare_handle(L)
+    rates = np.zeros(6, np.float64)
+    _check(L.cp_measure_primitives(device, rates.ctypes.data), "cp_measure_primitives")
+    return dict(zip(("dfma", "dadd_rd", "dmul_rd", "ddiv_rd", "asin", "ffma"), rates.tolist()))
+
+
+def _sizes4(sizes):
+    if sizes is None:
+        return None
+    return (ctypes.c_int32 * 4)(*(list(sizes) + [1] * (4 - len(sizes))))
+
+
+class Prover:
+    """A prover handle (device scratch, stream and counters) over the C ABI."""
+
+    def __init__(self, device: int = 0):
+        L = lib()
+        _declare_handle(L)
+        self._L = L
+        h = ctypes.c_void_p()
+        _check(L.cp_create(device, ctypes.byref(h)), "cp_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.cp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        """The handle's CUDA stream as a torch ExternalStream."""
+        torch = _torch()
+        return torch.cuda.ExternalStream(self._L.cp_get_stream(self._h))
+
+    def interrupt(self):
+        self._L.cp_request_interrupt(self._h)
+
+    @staticmethod
+    def opts(family, precision=FP64, policy=SPLIT_UNIFORM, max_depth=2, seed_sizes=None, seed_lambda=None,
+             level_capacity=0, learned_order=False) -> RefineOpts:
+        o = RefineOpts()
+        o.family, o.precision, o.policy, o.max_depth = family, precision, policy, max_depth
+        ss = list(seed_sizes or [64] * DIMS[family]) + [1] * 4
+        for d in range(4):
+            o.seed_sizes[d] = ss[d]
+        sl = seed_lambda or (LAMBDA_MIN, LAMBDA_MAX)
+        o.seed_lambda[0], o.seed_lambda[1] = sl
+        o.level_capacity = level_capacity
+        o.block = 0
+        o.learned_order = int(bool(learned_order))
+        return o
+
+    def autotune(self, family, **kw):
+        """Times every level-kernel variant on this refinement and keeps the fastest."""
+        o = self.opts(family, **kw)
+        best = ctypes.c_int()
+        ms = np.zeros(4, np.float64)
+        _check(self._L.cp_autotune(self._h, ctypes.byref(o), ctypes.byref(best), ms.ctypes.data), "cp_autotune")
+        return best.value, ms.tolist()
+
+    def set_level_variant(self, family, precision, variant):
+        _check(self._L.cp_set_level_variant(self._h, family, precision, variant), "cp_set_level_variant")
+
+    def refine(self, family, **kw) -> dict:
+        o = self.opts(family, **kw)
+        r = RefineReport()
+        _check(self._L.cp_refine(self._h, ctypes.byref(o), ctypes.byref(r)), "cp_refine")
+        return r.as_dict()
+
+    def refine_boxes(self, family, lo, hi, depth=None, **kw) -> dict:
+        """Refine explicit seed boxes: torch CUDA tensors (device) or numpy (host entry)."""
+        o = self.opts(family, **kw)
+        r = RefineReport()
+        if isinstance(lo, np.ndarray):
+            lo = np.ascontiguousarray(lo, np.float64)
+            hi = np.ascontiguousarray(hi, np.float64)
+            dp = np.ascontiguousarray(depth, np.uint8).ctypes.data if depth is not None else None
+            _check(self._L.cp_refine_boxes_host(self._h, ctypes.byref(o), lo.ctypes.data, hi.ctypes.data, dp,
+                                               lo.shape[1], ctypes.byref(r)), "cp_refine_boxes_host")
+        else:
+            torch = _torch()
+            lo = _dev(lo, torch.float64)
+            hi = _dev(hi, torch.float64)
+            dp = _dev(depth, torch.uint8) if depth is not None else None
+            torch.cuda.synchronize()
+            _check(self._L.cp_refine_boxes(self._h, ctypes.byref(o), _ptr(lo), _ptr(hi), _ptr(dp), lo.shape[1],
+                                          ctypes.byref(r)), "cp_refine_boxes")
+        return r.as_dict()
+
+    def reference_step(self, family, la_lb, la_ub, sizes=None):
+        """One reference-semantics lattice launch: smallest failing lambda.lb (inf if none)."""
+        first = ctypes.c_double()
+        err = (ctypes.c_double * 8)()
+        st = self._L.cp_reference_step(self._h, family, la_lb, la_ub, _sizes4(sizes), ctypes.byref(first), err)
+        if st != 0:
+            raise ProverError(st, f"cp_reference_step (box {list(err)})")
+        return first.value
+
+    def prove_family_reference(self, family, la_lb=LAMBDA_MIN, la_ub=LAMBDA_MAX, sizes=None, max_launches=0,
+                               trace_cap=0):
+        r = ReferenceReport()
+        trace = np.zeros((max(trace_cap, 1), 3), np.float64)
+        st = self._L.cp_prove_family_reference(self._h, family, la_lb, la_ub, _sizes4(sizes), max_launches,
+                                               trace.ctypes.data if trace_cap else None, ctypes.byref(r))
+        d = r.as_dict()
+        d["status"] = STATUS.get(st, st)
+        if trace_cap:
+            d["trace"] = trace[: min(r.launches, trace_cap)]
+        return d
+
+    def reference_criticals(self, family, la_lb, la_ub, sizes=None, max_boxes=1000):
+        boxes = np.zeros((max(max_boxes, 1), 8), np.float64)
+        handles = np.zeros(max(max_boxes, 1), np.uint8)
+        count = ctypes.c_size_t()
+        _check(self._L.cp_reference_criticals(self._h, family, la_lb, la_ub, _sizes4(sizes), max_boxes,
+                                             boxes.ctypes.data, handles.ctypes.data, ctypes.byref(count)),
+               "cp_reference_criticals")
+        m = min(count.value, max_boxes)
+        return count.value, boxes[:m], handles[:m]

@@ -1,0 +1,879 @@
+// Prover handle, box refinement (level stack) and the reference-semantics
+// lambda loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <queue>
+#include <vector>
+
+#include "cp_common.h"
+#include "cp_engine.h"
+#include "cp_fp32.cuh"
+#include "cp_worklist.cuh"
+
+using namespace cpb;
+
+namespace {
+
+// counter block layout (unsigned long long)
+enum : int {
+    C_VERDICT = 0,  // 5 verdict counts
+    C_UNRESOLVED = 5,
+    C_CLIPPED = 6,
+    C_FP32 = 7,
+    C_OUT = 8,      // children appended
+    C_ERR = 9,      // error flags
+    C_BEST_SLAB = 10,
+    C_EVALUATED = 11,
+    C_FIRST_BITS = 12,  // ordered encoding of the smallest failing lambda.lb
+    C_ERRBOX_CLAIM = 13,
+    C_ERRBOX = 14,      // 8 slots: lo/hi of the first erroneous box
+    C_COLLECT = 22,
+    C_NOFIT_SLAB = 23,  // smallest lambda slab holding a box whose fit check fired (middle/end)
+    C_TRAP_SLAB = 24,   // smallest lambda slab holding a box that reached a trap site
+    C_COUNT = 26
+};
+enum : unsigned long long { E_OVERFLOW = 1, E_NOFIT = 2, E_TRAP = 4 };
+constexpr int kDepthBins = 64;
+
+// order-preserving map of a double onto unsigned 64-bit (the encoding of
+// Atomic_ordered_double, atomic_float.hpp:56-66)
+__host__ __device__ __forceinline__ unsigned long long ordered_bits(double v) {
+    unsigned long long b;
+    memcpy(&b, &v, 8);
+    unsigned long long mask = (0ull - (b >> 63)) | (1ull << 63);
+    return b ^ mask;
+}
+__host__ __device__ __forceinline__ double ordered_value(unsigned long long u) {
+    unsigned long long mask = ((u >> 63) - 1) | (1ull << 63);
+    unsigned long long b = u ^ mask;
+    double v;
+    memcpy(&v, &b, 8);
+    return v;
+}
+
+struct LevelArgs {
+    BoxList in;
+    size_t begin, count;
+    BoxList out;
+    unsigned long long* cnt;
+    unsigned long long* per_depth;
+    SingleTable tab;
+    int policy, max_depth;
+    const uint8_t* axis_hint;   // per input box (SPLIT_GIVEN), indexed from `begin`
+    const uint8_t* order_hint;  // per input box criterion order, or null
+};
+
+// MINB: minimum resident blocks per SM requested from the compiler (register cap
+// 65536 / (128 * MINB)); the autotuner picks the variant per family and precision.
+template <int FAM, int PREC, int MINB>
+__global__ void __launch_bounds__(kEvalBlock, MINB) k_level(LevelArgs a) {
+    constexpr int D = family_dims(FAM);
+    __shared__ unsigned long long s_hist[8];
+    __shared__ unsigned long long s_depth[kDepthBins];
+    for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x) s_depth[t] = 0;
+    if (threadIdx.x < 8) s_hist[threadIdx.x] = 0;
+    __syncthreads();
+    const size_t step = (size_t)gridDim.x * blockDim.x;
+    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < a.count; base += step) {
+        const size_t j = base + threadIdx.x;
+        const size_t i = a.begin + j;
+        unsigned nchild = 0;
+        double lo[4], hi[4];
+        int depth = 0, axis = 0;
+        if (j < a.count) {
+            depth = a.in.depth[i];
+            if (depth == 0xFF) {
+                atomicAdd(&s_hist[C_CLIPPED], 1ull);
+            } else {
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    lo[d] = a.in.lo[d * a.in.cap + i];
+                    hi[d] = a.in.hi[d * a.in.cap + i];
+                }
+                const int ord = a.order_hint ? a.order_hint[j] : 0;
+                int v;
+                if (PREC == CP_FP32_PREFILTER) {
+                    uint8_t pmask;
+                    const int pre = prefilter_box<FAM>(lo, hi, ord, false, &pmask);
+                    if (pre == PF_UNDECIDED) {
+                        v = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr).verdict;
+                    } else {
+                        v = pre == PF_PROVED ? V_PROVED : pre == PF_EMPTY ? V_EMPTY : pre == PF_NOFIT ? V_NOFIT : V_CRITICAL;
+                        if (pre != PF_EMPTY) atomicAdd(&s_hist[C_FP32], 1ull);
+                    }
+                } else {
+                    v = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr).verdict;
+                }
+                atomicAdd(&s_hist[v], 1ull);
+                atomicAdd(&s_depth[depth < kDepthBins ? depth : kDepthBins - 1], 1ull);
+                if (v != V_PROVED && v != V_EMPTY) {
+                    if (depth >= a.max_depth) {
+                        atomicAdd(&s_hist[C_UNRESOLVED], 1ull);
+                    } else {
+                        nchild = fanout(a.policy, D);
+                        if (a.policy == SPLIT_WIDEST)
+                            axis = widest_axis<D>(lo, hi);
+                        else if (a.policy == SPLIT_GIVEN)
+                            axis = a.axis_hint ? (a.axis_hint[j] % D) : 0;
+                    }
+                }
+            }
+        }
+        const unsigned long long slot = warp_reserve(&a.cnt[C_OUT], nchild);
+        if (nchild) {
+            if (slot + nchild > a.out.cap) {
+                atomicOr(&a.cnt[C_ERR], E_OVERFLOW);
+            } else {
+                for (unsigned c = 0; c < nchild; ++c) {
+                    double clo[4], chi[4];
+                    make_child<D>(lo, hi, a.policy, axis, (int)c, clo, chi);
+                    const bool alive = clip_child<FAM>(clo, chi, a.tab);
+                    const size_t o = (size_t)(slot + c);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        a.out.lo[d * a.out.cap + o] = clo[d];
+                        a.out.hi[d * a.out.cap + o] = chi[d];
+                    }
+                    a.out.depth[o] = alive ? (uint8_t)(depth + 1) : (uint8_t)0xFF;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 8 && threadIdx.x != C_OUT && s_hist[threadIdx.x])
+        atomicAdd(&a.cnt[threadIdx.x], s_hist[threadIdx.x]);
+    for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x)
+        if (s_depth[t]) atomicAdd(&a.per_depth[t], s_depth[t]);
+}
+
+// Seed: every box of a family lattice, depth 0.
+__global__ void k_seed(LatticeSpec s, const double* __restrict__ slab_single, size_t total, BoxList out) {
+    const int D = family_dims(s.fam);
+    const size_t step = (size_t)gridDim.x * blockDim.x;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += step) {
+        size_t rem = t;
+        int ix[4] = {0, 0, 0, 0};
+        for (int d = D - 1; d >= 0; --d) {
+            ix[d] = (int)(rem % (size_t)s.n[d]);
+            rem /= (size_t)s.n[d];
+        }
+        double l[4], h[4];
+        const bool visited = lattice_box(s, ix, slab_single[ix[0]], l, h);
+        for (int d = 0; d < D; ++d) {
+            out.lo[d * out.cap + t] = l[d];
+            out.hi[d * out.cap + t] = h[d];
+        }
+        out.depth[t] = visited ? 0 : 0xFF;
+    }
+}
+
+__global__ void k_copy_seed(int dims, const double* __restrict__ lo, const double* __restrict__ hi,
+                            const uint8_t* __restrict__ depth, size_t n, BoxList out) {
+    const size_t step = (size_t)gridDim.x * blockDim.x;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += step) {
+        for (int d = 0; d < dims; ++d) {
+            out.lo[d * out.cap + t] = lo[d * n + t];
+            out.hi[d * out.cap + t] = hi[d * n + t];
+        }
+        out.depth[t] = depth ? depth[t] : 0;
+    }
+}
+
+__global__ void k_single_table(double lo, double h, int n, double* t, double* v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double x = __fma_rn((double)i, h, lo);
+        t[i] = x;
+        v[i] = single_placement(x);
+    }
+}
+
+// ------------------------------------------------------------------ reference step
+struct RefArgs {
+    LatticeSpec s;
+    const double* slab_single;
+    int slab_begin;
+    size_t count;  // boxes in this wave
+    unsigned long long* cnt;
+    int collect;  // 1: record every failing box (no early exit)
+    double* coll;
+    uint8_t* coll_handles;
+    size_t coll_cap;
+};
+
+// The body of the family kernels' loops (e.g. middle_configuration.cu:157-201)
+// over the lattice boxes of lambda slabs [slab_begin, ...), stopping at slabs
+// beyond the first slab that holds a failing box.
+template <int FAM>
+__global__ void __launch_bounds__(kEvalBlock) k_ref_step(RefArgs a) {
+    constexpr int D = family_dims(FAM);
+    size_t per_slab = 1;
+    for (int d = 1; d < D; ++d) per_slab *= (size_t)a.s.n[d];
+    const size_t step = (size_t)gridDim.x * blockDim.x;
+    unsigned long long evaluated = 0;
+    volatile unsigned long long* best = a.cnt + C_BEST_SLAB;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.count; t += step) {
+        const int slab = a.slab_begin + (int)(t / per_slab);
+        if (!a.collect && (unsigned long long)slab > *best) continue;
+        size_t rem = t % per_slab;
+        int ix[4] = {slab, 0, 0, 0};
+        for (int d = D - 1; d >= 1; --d) {
+            ix[d] = (int)(rem % (size_t)a.s.n[d]);
+            rem /= (size_t)a.s.n[d];
+        }
+        double lo[4], hi[4];
+        if (!lattice_box(a.s, ix, a.slab_single[slab], lo, hi)) continue;
+        ++evaluated;
+        Verdict v = a.collect ? eval_box<FAM, FULL>(lo, hi, 0, nullptr) : eval_box<FAM, DECIDE>(lo, hi, 0, nullptr);
+        if (v.verdict == V_EMPTY) continue;
+        const bool nofit = (v.mask & M_FIT) && FAM != F_START && FAM != F_START_END_2D && FAM != F_START_END_3D;
+        const bool trap = (v.mask & M_TRAP) != 0;
+        if (nofit || trap) {
+            atomicMin(&a.cnt[trap ? C_TRAP_SLAB : C_NOFIT_SLAB], (unsigned long long)slab);
+            if (atomicCAS(&a.cnt[C_ERRBOX_CLAIM], 0ull, 1ull) == 0ull) {
+                for (int d = 0; d < D; ++d) {
+                    a.cnt[C_ERRBOX + 2 * d] = __double_as_longlong(lo[d]);
+                    a.cnt[C_ERRBOX + 2 * d + 1] = __double_as_longlong(hi[d]);
+                }
+            }
+        }
+        if (v.mask & M_CRIT) {
+            atomicMin(&a.cnt[C_BEST_SLAB], (unsigned long long)slab);
+            atomicMin(&a.cnt[C_FIRST_BITS], ordered_bits(lo[0]));
+            if (a.collect) {
+                const unsigned long long k = atomicAdd(&a.cnt[C_COLLECT], 1ull);
+                if (k < a.coll_cap) {
+                    // the box as the reference prints it: r2, r1 tightened
+                    if (D == 4 && lo[2] < lo[3]) lo[2] = lo[3];
+                    if (lo[1] < lo[2]) lo[1] = lo[2];
+                    double* rec = a.coll + 8 * k;
+                    for (int d = 0; d < 4; ++d) {
+                        rec[2 * d] = d < D ? lo[d] : 0.0;
+                        rec[2 * d + 1] = d < D ? hi[d] : 0.0;
+                    }
+                    uint8_t hb = v.mask & M_CRIT;
+                    if (FAM == F_MIDDLE) hb = (uint8_t)(((hb & 3) ? 1 : 0) | ((hb & 12) ? 2 : 0));
+                    a.coll_handles[k] = hb;
+                }
+            }
+        }
+    }
+    if (evaluated) atomicAdd(&a.cnt[C_EVALUATED], evaluated);
+}
+
+template <class K>
+unsigned grid_of(K kernel, int block) {
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return (unsigned)(sms * per_sm);
+}
+
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ handle
+struct LevelBuf {
+    BoxList b{nullptr, nullptr, nullptr, 0};
+    size_t n = 0;
+};
+
+struct cp_prover {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::atomic<int> interrupt{0};
+    unsigned long long* cnt = nullptr;  // C_COUNT counters
+    unsigned long long* per_depth = nullptr;
+    unsigned long long* h_cnt = nullptr;  // pinned mirror
+    double* tab_t = nullptr;
+    double* tab_v = nullptr;
+    int tab_n = 0;
+    double tab_h = 0;
+    double* slab_single = nullptr;
+    int slab_cap = 0;
+    std::vector<LevelBuf> levels;
+    int levels_dims = 0;
+    size_t level_cap = 0;
+    void* model = nullptr;  // learned model state (cp_model.cu)
+    int variant[6][2] = {{1, 1}, {0, 0}, {1, 1}, {1, 1}, {0, 0}, {1, 1}};  // level-kernel variant per family/precision
+};
+
+cudaStream_t cp_prover_stream(cp_prover* p) { return p->stream; }
+void*& cp_prover_model(cp_prover* p) { return p->model; }
+
+namespace {
+
+cp_status cuda_ok(cudaError_t e, cp_status s = CP_ERR_CUDA) {
+    if (e == cudaSuccess) return CP_OK;
+    return cp_record_cuda_error(e, e == cudaErrorMemoryAllocation ? CP_ERR_NOMEM : s);
+}
+#define CP_TRY(x)                      \
+    do {                               \
+        cp_status s_ = (x);            \
+        if (s_ != CP_OK) return s_;    \
+    } while (0)
+
+cp_status reset_counters(cp_prover* p) {
+    CP_TRY(cuda_ok(cudaMemsetAsync(p->cnt, 0, sizeof(unsigned long long) * C_COUNT, p->stream)));
+    return cuda_ok(cudaMemsetAsync(p->per_depth, 0, sizeof(unsigned long long) * kDepthBins, p->stream));
+}
+
+cp_status read_counters(cp_prover* p) {
+    CP_TRY(cuda_ok(cudaMemcpyAsync(p->h_cnt, p->cnt, sizeof(unsigned long long) * (C_COUNT + kDepthBins),
+                                   cudaMemcpyDeviceToHost, p->stream)));
+    return cuda_ok(cudaStreamSynchronize(p->stream));
+}
+
+void free_levels(cp_prover* p) {
+    for (auto& L : p->levels) {
+        cudaFree(L.b.lo);
+        cudaFree(L.b.hi);
+        cudaFree(L.b.depth);
+    }
+    p->levels.clear();
+}
+
+cp_status ensure_levels(cp_prover* p, int count, int dims, size_t cap) {
+    if ((int)p->levels.size() >= count && p->levels_dims >= dims && p->level_cap == cap) return CP_OK;
+    if (p->levels_dims < dims || p->level_cap != cap) free_levels(p);
+    p->levels_dims = dims;
+    p->level_cap = cap;
+    while ((int)p->levels.size() < count) {
+        LevelBuf L;
+        L.b.cap = cap;
+        CP_TRY(cuda_ok(cudaMalloc(&L.b.lo, sizeof(double) * dims * cap)));
+        CP_TRY(cuda_ok(cudaMalloc(&L.b.hi, sizeof(double) * dims * cap)));
+        CP_TRY(cuda_ok(cudaMalloc(&L.b.depth, cap)));
+        p->levels.push_back(L);
+    }
+    return CP_OK;
+}
+
+cp_status ensure_slab(cp_prover* p, int n) {
+    if (p->slab_cap >= n) return CP_OK;
+    cudaFree(p->slab_single);
+    p->slab_single = nullptr;
+    p->slab_cap = 0;
+    CP_TRY(cuda_ok(cudaMalloc(&p->slab_single, sizeof(double) * n)));
+    p->slab_cap = n;
+    return CP_OK;
+}
+
+SingleTable table_of(const cp_prover* p) { return SingleTable{p->tab_t, p->tab_v, p->tab_n, p->tab_h}; }
+
+using LevelKernel = void (*)(LevelArgs);
+constexpr int kVariants = 4;
+constexpr int kVariantMinBlocks[kVariants] = {1, 4, 5, 6};
+template <int FAM, int PREC>
+LevelKernel level_variant(int v) {
+    switch (v) {
+    case 1: return k_level<FAM, PREC, 4>;
+    case 2: return k_level<FAM, PREC, 5>;
+    case 3: return k_level<FAM, PREC, 6>;
+    default: return k_level<FAM, PREC, 1>;
+    }
+}
+template <int FAM>
+LevelKernel level_variant_p(int prec, int v) {
+    return prec ? level_variant<FAM, 1>(v) : level_variant<FAM, 0>(v);
+}
+LevelKernel level_kernel(int fam, int prec, int v) {
+    switch (fam) {
+    case 0: return level_variant_p<0>(prec, v);
+    case 1: return level_variant_p<1>(prec, v);
+    case 2: return level_variant_p<2>(prec, v);
+    case 3: return level_variant_p<3>(prec, v);
+    case 4: return level_variant_p<4>(prec, v);
+    default: return level_variant_p<5>(prec, v);
+    }
+}
+
+using RefKernel = void (*)(RefArgs);
+RefKernel ref_kernel(int fam) {
+    static const RefKernel k[6] = {k_ref_step<0>, k_ref_step<1>, k_ref_step<2>,
+                                   k_ref_step<3>, k_ref_step<4>, k_ref_step<5>};
+    return k[fam];
+}
+
+// the reference's lattice sizes per family (start_configuration.cu:41-53,
+// middle_configuration.cu:39-42, end_configuration.cu:39-49)
+void reference_sizes(int fam, int* n) {
+    static const int s[6][4] = {{256, 256, 256, 64}, {4096, 4096, 4096, 1}, {256, 256, 256, 64},
+                                {512, 256, 256, 64}, {4096, 1024, 1024, 1}, {1024, 256, 128, 128}};
+    for (int d = 0; d < 4; ++d) n[d] = s[fam][d];
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ internal API
+cp_status cp_engine_eval_chunk(cp_prover* p, int fam, const cp_refine_opts& o, LevelBuf& in, size_t begin,
+                               size_t count, LevelBuf* out, const uint8_t* axis_hint, const uint8_t* order_hint,
+                               double* ms) {
+    LevelArgs a;
+    a.in = in.b;
+    a.begin = begin;
+    a.count = count;
+    a.out = out ? out->b : BoxList{nullptr, nullptr, nullptr, 0};
+    a.cnt = p->cnt;
+    a.per_depth = p->per_depth;
+    a.tab = table_of(p);
+    a.policy = o.policy == CP_SPLIT_LEARNED ? SPLIT_GIVEN : o.policy;
+    a.max_depth = out ? o.max_depth : 0;
+    a.axis_hint = axis_hint;
+    a.order_hint = order_hint;
+    // children append after the boxes already in `out`
+    unsigned long long base = out ? out->n : 0;
+    CP_TRY(cuda_ok(cudaMemcpyAsync(p->cnt + C_OUT, &base, sizeof(base), cudaMemcpyHostToDevice, p->stream)));
+    LevelKernel k = level_kernel(fam, o.precision, p->variant[fam][o.precision ? 1 : 0]);
+    const int block = kEvalBlock;
+    unsigned grid = grid_of(k, block);
+    size_t need = (count + block - 1) / block;
+    if (need < grid) grid = (unsigned)std::max<size_t>(need, 1);
+    cudaEventRecord(p->ev0, p->stream);
+    k<<<grid, block, 0, p->stream>>>(a);
+    cudaEventRecord(p->ev1, p->stream);
+    CP_TRY(cp_check_launch());
+    CP_TRY(read_counters(p));
+    float t = 0;
+    cudaEventElapsedTime(&t, p->ev0, p->ev1);
+    *ms += t;
+    if (p->h_cnt[C_ERR] & E_OVERFLOW) return CP_ERR_CAPACITY;
+    if (out) out->n = (size_t)p->h_cnt[C_OUT];
+    return CP_OK;
+}
+
+namespace {
+
+cp_status refine_levels(cp_prover* p, const cp_refine_opts& o, cp_refine_report* r, double t_wall0) {
+    const int fam = o.family;
+    const int D = family_dims(fam);
+    const int F = fanout(o.policy == CP_SPLIT_LEARNED ? SPLIT_GIVEN : o.policy, D);
+    double ms = 0;
+    int launches = 0;
+    const int L = o.max_depth;
+    for (;;) {
+        int l = -1;
+        for (int k = (int)p->levels.size() - 1; k >= 0; --k)
+            if (p->levels[k].n > 0) {
+                l = k;
+                break;
+            }
+        if (l < 0) break;
+        LevelBuf& in = p->levels[l];
+        LevelBuf* out = (l + 1 < (int)p->levels.size() && l < L) ? &p->levels[l + 1] : nullptr;
+        size_t c;
+        if (out) {
+            size_t free_slots = out->b.cap - out->n;
+            c = std::min(in.n, free_slots / (size_t)F);
+            if (c == 0) return CP_ERR_CAPACITY;
+        } else {
+            c = in.n;
+        }
+        const size_t begin = in.n - c;
+        uint8_t *axis = nullptr, *order = nullptr;
+        if (o.policy == CP_SPLIT_LEARNED || o.learned_order) {
+            CP_TRY(cp_model_hints(p, fam, in.b, begin, c, o.policy == CP_SPLIT_LEARNED ? &axis : nullptr,
+                                  o.learned_order ? &order : nullptr));
+        }
+        CP_TRY(cp_engine_eval_chunk(p, fam, o, in, begin, c, out, axis, order, &ms));
+        ++launches;
+        in.n -= c;
+        if (p->interrupt.load()) {
+            p->interrupt.store(0);
+            return CP_ERR_INTERRUPTED;
+        }
+    }
+    (void)D;
+    r->launches = launches;
+    r->device_ms = ms;
+    for (int v = 0; v < 5; ++v) r->verdicts[v] = (int64_t)p->h_cnt[C_VERDICT + v];
+    r->unresolved = (int64_t)p->h_cnt[C_UNRESOLVED];
+    r->clipped = (int64_t)p->h_cnt[C_CLIPPED];
+    r->fp32_decided = (int64_t)p->h_cnt[C_FP32];
+    r->evaluated = 0;
+    for (int v = 0; v < 5; ++v) r->evaluated += r->verdicts[v];
+    r->max_depth_seen = 0;
+    for (int d = 0; d < kDepthBins; ++d) {
+        r->per_depth[d] = (int64_t)p->h_cnt[C_COUNT + d];
+        if (r->per_depth[d]) r->max_depth_seen = d;
+    }
+    r->wall_ms = now_ms() - t_wall0;
+    return CP_OK;
+}
+
+cp_status check_opts(const cp_refine_opts* o) {
+    if (!o || o->family < 0 || o->family > 5) return CP_ERR_INVALID;
+    if (o->precision != CP_FP64 && o->precision != CP_FP32_PREFILTER) return CP_ERR_INVALID;
+    if (o->policy < CP_SPLIT_UNIFORM || o->policy > CP_SPLIT_LEARNED) return CP_ERR_INVALID;
+    if (o->max_depth < 0 || o->max_depth > 250) return CP_ERR_INVALID;
+    return CP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cp_status cp_create(int device, cp_prover** out) {
+    if (!out) return CP_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return CP_ERR_NO_DEVICE;
+    }
+    CP_TRY(cuda_ok(cudaSetDevice(device)));
+    cp_prover* p = new cp_prover();
+    p->device = device;
+    cp_status s = CP_OK;
+    do {
+        if ((s = cuda_ok(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking))) != CP_OK) break;
+        if ((s = cuda_ok(cudaEventCreate(&p->ev0))) != CP_OK) break;
+        if ((s = cuda_ok(cudaEventCreate(&p->ev1))) != CP_OK) break;
+        if ((s = cuda_ok(cudaMalloc(&p->cnt, sizeof(unsigned long long) * (C_COUNT + kDepthBins)))) != CP_OK) break;
+        p->per_depth = p->cnt + C_COUNT;
+        if ((s = cuda_ok(cudaMallocHost(&p->h_cnt, sizeof(unsigned long long) * (C_COUNT + kDepthBins)))) != CP_OK)
+            break;
+        // single-placement table on 2^16 lambda points over [0.5, 0.99]
+        p->tab_n = 1 << 16;
+        p->tab_h = (kLambdaMax - kLambdaMin) / (p->tab_n - 1);
+        if ((s = cuda_ok(cudaMalloc(&p->tab_t, sizeof(double) * p->tab_n))) != CP_OK) break;
+        if ((s = cuda_ok(cudaMalloc(&p->tab_v, sizeof(double) * p->tab_n))) != CP_OK) break;
+        k_single_table<<<256, 128, 0, p->stream>>>(kLambdaMin, p->tab_h, p->tab_n, p->tab_t, p->tab_v);
+        if ((s = cp_check_launch()) != CP_OK) break;
+        if ((s = cuda_ok(cudaStreamSynchronize(p->stream))) != CP_OK) break;
+    } while (0);
+    if (s != CP_OK) {
+        cp_destroy(p);
+        return s;
+    }
+    *out = p;
+    return CP_OK;
+}
+
+void cp_destroy(cp_prover* p) {
+    if (!p) return;
+    cudaSetDevice(p->device);
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    cp_model_free(p);
+    free_levels(p);
+    cudaFree(p->cnt);
+    cudaFreeHost(p->h_cnt);
+    cudaFree(p->tab_t);
+    cudaFree(p->tab_v);
+    cudaFree(p->slab_single);
+    if (p->ev0) cudaEventDestroy(p->ev0);
+    if (p->ev1) cudaEventDestroy(p->ev1);
+    if (p->stream) cudaStreamDestroy(p->stream);
+    delete p;
+}
+
+void* cp_get_stream(cp_prover* p) { return p ? (void*)p->stream : nullptr; }
+
+void cp_request_interrupt(cp_prover* p) {
+    if (p) p->interrupt.store(1);
+}
+
+cp_status cp_refine(cp_prover* p, const cp_refine_opts* o, cp_refine_report* r) {
+    if (!p || !r) return CP_ERR_INVALID;
+    CP_TRY(check_opts(o));
+    const double t0 = now_ms();
+    std::memset(r, 0, sizeof(*r));
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    const int fam = o->family;
+    const int D = family_dims(fam);
+    LatticeSpec s{fam, {1, 1, 1, 1}, o->seed_lambda[0], o->seed_lambda[1]};
+    size_t total = 1;
+    for (int d = 0; d < D; ++d) {
+        if (o->seed_sizes[d] <= 0) return CP_ERR_INVALID;
+        s.n[d] = o->seed_sizes[d];
+        total *= (size_t)s.n[d];
+    }
+    const size_t cap = o->level_capacity > 0 ? (size_t)o->level_capacity : ((size_t)1 << 25);
+    if (total > cap) return CP_ERR_CAPACITY;
+    CP_TRY(ensure_levels(p, o->max_depth + 1, D, cap));
+    for (auto& L : p->levels) L.n = 0;
+    CP_TRY(ensure_slab(p, s.n[0]));
+    CP_TRY(cp_launch_slab_single(s, p->slab_single, p->stream));
+    k_seed<<<grid_of(k_seed, 128), 128, 0, p->stream>>>(s, p->slab_single, total, p->levels[0].b);
+    CP_TRY(cp_check_launch());
+    p->levels[0].n = total;
+    CP_TRY(reset_counters(p));
+    return refine_levels(p, *o, r, t0);
+}
+
+cp_status cp_set_level_variant(cp_prover* p, int family, int precision, int variant) {
+    if (!p || family < 0 || family > 5 || precision < 0 || precision > 1 || variant < 0 || variant >= kVariants)
+        return CP_ERR_INVALID;
+    p->variant[family][precision] = variant;
+    return CP_OK;
+}
+
+cp_status cp_autotune(cp_prover* p, const cp_refine_opts* o, int* best, double* ms) {
+    if (!p || !best) return CP_ERR_INVALID;
+    CP_TRY(check_opts(o));
+    const int pr = o->precision ? 1 : 0;
+    double best_ms = 1e300;
+    int best_v = 0;
+    for (int v = 0; v < kVariants; ++v) {
+        p->variant[o->family][pr] = v;
+        cp_refine_report r;
+        CP_TRY(cp_refine(p, o, &r));  // warm-up
+        CP_TRY(cp_refine(p, o, &r));
+        if (ms) ms[v] = r.device_ms;
+        if (r.device_ms < best_ms) {
+            best_ms = r.device_ms;
+            best_v = v;
+        }
+    }
+    p->variant[o->family][pr] = best_v;
+    *best = best_v;
+    return CP_OK;
+}
+
+cp_status cp_refine_boxes(cp_prover* p, const cp_refine_opts* o, const double* lo, const double* hi,
+                          const uint8_t* depth, size_t n, cp_refine_report* r) {
+    if (!p || !r || (n && (!lo || !hi))) return CP_ERR_INVALID;
+    CP_TRY(check_opts(o));
+    const double t0 = now_ms();
+    std::memset(r, 0, sizeof(*r));
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    const int D = family_dims(o->family);
+    const size_t cap = o->level_capacity > 0 ? (size_t)o->level_capacity : ((size_t)1 << 25);
+    if (n > cap) return CP_ERR_CAPACITY;
+    CP_TRY(ensure_levels(p, o->max_depth + 1, D, cap));
+    for (auto& L : p->levels) L.n = 0;
+    if (n) {
+        k_copy_seed<<<grid_of(k_copy_seed, 128), 128, 0, p->stream>>>(D, lo, hi, depth, n, p->levels[0].b);
+        CP_TRY(cp_check_launch());
+    }
+    p->levels[0].n = n;
+    CP_TRY(reset_counters(p));
+    // explicit seeds may carry depths above zero: they stay in level 0's buffer
+    // and their children go to level 1; max_depth compares with the box depth
+    return refine_levels(p, *o, r, t0);
+}
+
+cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* o, const double* lo, const double* hi,
+                               const uint8_t* depth, size_t n, cp_refine_report* r) {
+    if (!p || !r || (n && (!lo || !hi))) return CP_ERR_INVALID;
+    CP_TRY(check_opts(o));
+    const double t0 = now_ms();
+    std::memset(r, 0, sizeof(*r));
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    const int D = family_dims(o->family);
+    const size_t cap = o->level_capacity > 0 ? (size_t)o->level_capacity : ((size_t)1 << 25);
+    if (n > cap) return CP_ERR_CAPACITY;
+    CP_TRY(ensure_levels(p, o->max_depth + 1, D, cap));
+    for (auto& L : p->levels) L.n = 0;
+    BoxList& b = p->levels[0].b;
+    for (int d = 0; d < D && n; ++d) {
+        CP_TRY(cuda_ok(cudaMemcpyAsync(b.lo + d * b.cap, lo + d * n, sizeof(double) * n, cudaMemcpyHostToDevice, p->stream)));
+        CP_TRY(cuda_ok(cudaMemcpyAsync(b.hi + d * b.cap, hi + d * n, sizeof(double) * n, cudaMemcpyHostToDevice, p->stream)));
+    }
+    if (n) {
+        if (depth)
+            CP_TRY(cuda_ok(cudaMemcpyAsync(b.depth, depth, n, cudaMemcpyHostToDevice, p->stream)));
+        else
+            CP_TRY(cuda_ok(cudaMemsetAsync(b.depth, 0, n, p->stream)));
+    }
+    p->levels[0].n = n;
+    CP_TRY(reset_counters(p));
+    return refine_levels(p, *o, r, t0);
+}
+
+cp_status cp_reference_step(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,
+                            double* first_critical, double* err_box) {
+    if (!p || family < 0 || family > 5 || !first_critical) return CP_ERR_INVALID;
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    const int D = family_dims(family);
+    LatticeSpec s{family, {1, 1, 1, 1}, la_lb, la_ub};
+    int rs[4];
+    reference_sizes(family, rs);
+    for (int d = 0; d < D; ++d) {
+        s.n[d] = sizes ? sizes[d] : rs[d];
+        if (s.n[d] <= 0) return CP_ERR_INVALID;
+    }
+    CP_TRY(ensure_slab(p, s.n[0]));
+    CP_TRY(cp_launch_slab_single(s, p->slab_single, p->stream));
+    CP_TRY(reset_counters(p));
+    const unsigned long long none = (unsigned long long)s.n[0], no_bits = ~0ull;
+    CP_TRY(cuda_ok(cudaMemcpyAsync(p->cnt + C_BEST_SLAB, &none, sizeof(none), cudaMemcpyHostToDevice, p->stream)));
+    CP_TRY(cuda_ok(cudaMemcpyAsync(p->cnt + C_NOFIT_SLAB, &none, sizeof(none), cudaMemcpyHostToDevice, p->stream)));
+    CP_TRY(cuda_ok(cudaMemcpyAsync(p->cnt + C_TRAP_SLAB, &none, sizeof(none), cudaMemcpyHostToDevice, p->stream)));
+    CP_TRY(cuda_ok(cudaMemcpyAsync(p->cnt + C_FIRST_BITS, &no_bits, sizeof(no_bits), cudaMemcpyHostToDevice, p->stream)));
+    CP_TRY(cuda_ok(cudaStreamSynchronize(p->stream)));
+    size_t per_slab = 1;
+    for (int d = 1; d < D; ++d) per_slab *= (size_t)s.n[d];
+    const size_t wave_boxes = (size_t)1 << 23;
+    const int wave_slabs = (int)std::max<size_t>(1, wave_boxes / per_slab);
+    RefKernel k = ref_kernel(family);
+    const unsigned grid = grid_of(k, kEvalBlock);
+    for (int s0 = 0; s0 < s.n[0]; s0 += wave_slabs) {
+        const int ns = std::min(wave_slabs, s.n[0] - s0);
+        RefArgs a{s, p->slab_single, s0, (size_t)ns * per_slab, p->cnt, 0, nullptr, nullptr, 0};
+        k<<<grid, kEvalBlock, 0, p->stream>>>(a);
+        CP_TRY(cp_check_launch());
+        CP_TRY(read_counters(p));
+        const unsigned long long stop = (unsigned long long)(s0 + ns - 1);
+        if (p->h_cnt[C_BEST_SLAB] < (unsigned long long)s.n[0] || p->h_cnt[C_TRAP_SLAB] <= stop ||
+            p->h_cnt[C_NOFIT_SLAB] <= stop)
+            break;
+    }
+    // Every box of the slabs up to the first failing slab was evaluated.  The
+    // reference kernel visits each thread's boxes lambda slab by lambda slab and
+    // returns at the thread's first failing box, so it certainly reaches (and
+    // traps on) a box of a slab below the first failing slab, or of any slab when
+    // no box fails; in the first failing slab itself that depends on its thread
+    // order, and later slabs are not evaluated here.  The certain cases are errors.
+    const unsigned long long best = p->h_cnt[C_BEST_SLAB];  // == n[0] when no box fails
+    const bool trap_hit = p->h_cnt[C_TRAP_SLAB] < best, nofit_hit = p->h_cnt[C_NOFIT_SLAB] < best;
+    if (err_box && (trap_hit || nofit_hit) && p->h_cnt[C_ERRBOX_CLAIM]) {
+        for (int j = 0; j < 8; ++j) {
+            unsigned long long b = p->h_cnt[C_ERRBOX + j];
+            std::memcpy(&err_box[j], &b, 8);
+        }
+    }
+    if (trap_hit) return CP_ERR_TRAP_SITE;
+    if (nofit_hit) return CP_ERR_NOFIT;
+    *first_critical = p->h_cnt[C_FIRST_BITS] == ~0ull ? INFINITY : ordered_value(p->h_cnt[C_FIRST_BITS]);
+    return CP_OK;
+}
+
+cp_status cp_prove_family_reference(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,
+                                    int64_t max_launches, double* trace, cp_reference_report* r) {
+    if (!p || !r || family < 0 || family > 5) return CP_ERR_INVALID;
+    std::memset(r, 0, sizeof(*r));
+    const double t0 = now_ms();
+    struct Lb {
+        bool operator()(const std::pair<double, double>& a, const std::pair<double, double>& b) const {
+            return a.first > b.first;
+        }
+    };
+    std::priority_queue<std::pair<double, double>, std::vector<std::pair<double, double>>, Lb> q;
+    q.push({la_lb, la_ub});
+    p->interrupt.store(0);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cp_status status = CP_OK;
+    while (!q.empty()) {
+        if (max_launches > 0 && r->launches >= max_launches) {
+            status = CP_ERR_NOT_PROVED;
+            break;
+        }
+        const auto cur = q.top();
+        q.pop();
+        double first = INFINITY;
+        cudaEventRecord(e0, p->stream);
+        cp_status s = cp_reference_step(p, family, cur.first, cur.second, sizes, &first, nullptr);
+        cudaEventRecord(e1, p->stream);
+        cudaEventSynchronize(e1);
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        r->device_ms += t;
+        r->boxes_evaluated += (int64_t)p->h_cnt[C_EVALUATED];
+        if (trace) {
+            trace[3 * r->launches + 0] = cur.first;
+            trace[3 * r->launches + 1] = cur.second;
+            trace[3 * r->launches + 2] = first;
+        }
+        r->launches++;
+        if (s != CP_OK) {
+            r->remaining[0] = cur.first;
+            r->remaining[1] = cur.second;
+            status = s;
+            break;
+        }
+        if (p->interrupt.load()) {
+            p->interrupt.store(0);
+            r->interrupted = 1;
+            if (first != INFINITY) {
+                r->remaining[0] = cur.first, r->remaining[1] = cur.second;
+            } else if (!q.empty()) {
+                r->remaining[0] = q.top().first, r->remaining[1] = q.top().second;
+            } else {
+                r->proved = 1;
+                break;
+            }
+            status = CP_ERR_INTERRUPTED;
+            break;
+        }
+        // run_kernel.cuh:110-127
+        if (first != INFINITY) {
+            const double width_before = cur.second - cur.first;
+            const double width_after = cur.second - first;
+            if (width_before >= 2 * width_after) {
+                q.push({first, cur.second});
+            } else {
+                const double mid = 0.5 * (first + cur.second);
+                if (first < mid) q.push({first, mid});
+                if (mid <= cur.second) q.push({mid, cur.second});
+            }
+        }
+    }
+    if (status == CP_OK) r->proved = 1;
+    if (status == CP_ERR_NOT_PROVED && !q.empty()) {
+        r->remaining[0] = q.top().first;
+        r->remaining[1] = q.top().second;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    r->wall_ms = now_ms() - t0;
+    return status;
+}
+
+cp_status cp_reference_criticals(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,
+                                 size_t max_boxes, double* boxes, uint8_t* handles, size_t* count) {
+    if (!p || family < 0 || family > 5 || !count || (max_boxes && (!boxes || !handles))) return CP_ERR_INVALID;
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    const int D = family_dims(family);
+    LatticeSpec s{family, {1, 1, 1, 1}, la_lb, la_ub};
+    int rs[4];
+    reference_sizes(family, rs);
+    for (int d = 0; d < D; ++d) {
+        s.n[d] = sizes ? sizes[d] : rs[d];
+        if (s.n[d] <= 0) return CP_ERR_INVALID;
+    }
+    CP_TRY(ensure_slab(p, s.n[0]));
+    CP_TRY(cp_launch_slab_single(s, p->slab_single, p->stream));
+    CP_TRY(reset_counters(p));
+    double* dboxes = nullptr;
+    uint8_t* dh = nullptr;
+    const size_t cap = max_boxes ? max_boxes : 1;
+    CP_TRY(cuda_ok(cudaMalloc(&dboxes, sizeof(double) * 8 * cap)));
+    if (cuda_ok(cudaMalloc(&dh, cap)) != CP_OK) {
+        cudaFree(dboxes);
+        return CP_ERR_NOMEM;
+    }
+    size_t per_slab = 1;
+    for (int d = 1; d < D; ++d) per_slab *= (size_t)s.n[d];
+    RefKernel k = ref_kernel(family);
+    RefArgs a{s, p->slab_single, 0, (size_t)s.n[0] * per_slab, p->cnt, 1, dboxes, dh, max_boxes};
+    k<<<grid_of(k, kEvalBlock), kEvalBlock, 0, p->stream>>>(a);
+    cp_status st = cp_check_launch();
+    if (st == CP_OK) st = read_counters(p);
+    if (st == CP_OK) {
+        *count = (size_t)p->h_cnt[C_COLLECT];
+        const size_t m = std::min(*count, max_boxes);
+        if (m) {
+            st = cuda_ok(cudaMemcpy(boxes, dboxes, sizeof(double) * 8 * m, cudaMemcpyDeviceToHost));
+            if (st == CP_OK) st = cuda_ok(cudaMemcpy(handles, dh, m, cudaMemcpyDeviceToHost));
+        }
+    }
+    cudaFree(dboxes);
+    cudaFree(dh);
+    return st;
+}
+
+}  // extern "C"

@@ -55,14 +55,14 @@ __global__ void __launch_bounds__(kEvalBlock) k_eval_prefilter(const double* __r
             h[d] = __ldg(hi + d * stride + i);
         }
         const int ord = order ? order[i] : 0;
-        const int pre = prefilter_box<FAM>(l, h);
+        uint8_t pmask = 0;
+        const int pre = prefilter_box<FAM>(l, h, ord, MODE == FULL, &pmask);
         Verdict v;
-        if (pre == PF_PROVED)
-            v = {V_PROVED, 0};
-        else if (pre == PF_EMPTY)
-            v = {V_EMPTY, 0};
-        else
+        if (pre == PF_UNDECIDED)
             v = eval_box<FAM, MODE>(l, h, ord, trace ? trace + 16 * i : nullptr);
+        else
+            v = {pre == PF_PROVED ? V_PROVED : pre == PF_EMPTY ? V_EMPTY : pre == PF_NOFIT ? V_NOFIT : V_CRITICAL,
+                 pmask};
         verdict[i] = v.verdict;
         mask[i] = v.mask;
     }
@@ -80,7 +80,8 @@ __global__ void k_slab_single(LatticeSpec s, double* __restrict__ out) {
 }
 
 __global__ void k_lattice(LatticeSpec s, const double* __restrict__ slab_single, const int64_t* __restrict__ index,
-                          size_t n, double* __restrict__ lo, double* __restrict__ hi, size_t stride) {
+                          size_t n, double* __restrict__ lo, double* __restrict__ hi, size_t stride,
+                          uint8_t* __restrict__ visited) {
     const int D = family_dims(s.fam);
     const size_t step = (size_t)gridDim.x * blockDim.x;
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += step) {
@@ -91,11 +92,12 @@ __global__ void k_lattice(LatticeSpec s, const double* __restrict__ slab_single,
             rem /= s.n[d];
         }
         double l[4], h[4];
-        lattice_box(s, ix, slab_single[ix[0]], l, h);
+        const bool v = lattice_box(s, ix, slab_single[ix[0]], l, h);
         for (int d = 0; d < D; ++d) {
             lo[d * stride + t] = l[d];
             hi[d * stride + t] = h[d];
         }
+        if (visited) visited[t] = v ? 1 : 0;
     }
 }
 
@@ -255,7 +257,7 @@ cp_status cp_eval_boxes_host(int family, int precision, int mode, const double* 
 }
 
 cp_status cp_lattice_boxes(int family, double outer_lb, double outer_ub, const int32_t* sizes, const int64_t* index,
-                           size_t n, double* lo, double* hi, size_t stride, void* stream) {
+                           size_t n, double* lo, double* hi, size_t stride, uint8_t* visited, void* stream) {
     if (family < 0 || family > 5 || !sizes || stride < n) return CP_ERR_INVALID;
     const int D = family_dims(family);
     LatticeSpec s{family, {1, 1, 1, 1}, outer_lb, outer_ub};
@@ -271,7 +273,7 @@ cp_status cp_lattice_boxes(int family, double outer_lb, double outer_ub, const i
     if (e != cudaSuccess) return cp_record_cuda_error(e, CP_ERR_NOMEM);
     cp_status rc = cp_launch_slab_single(s, slab, st);
     if (rc == CP_OK) {
-        k_lattice<<<grid_for(k_lattice, n, 128), 128, 0, st>>>(s, slab, index, n, lo, hi, stride);
+        k_lattice<<<grid_for(k_lattice, n, 128), 128, 0, st>>>(s, slab, index, n, lo, hi, stride, visited);
         rc = cp_check_launch();
     }
     cudaFreeAsync(slab, st);

@@ -55,7 +55,10 @@ struct LatticeSpec {
 };
 
 // Raw box at lattice coordinates ix; `single` = single placement bound of la.lo.
-__device__ __forceinline__ void lattice_box(const LatticeSpec& s, const int* ix, double single, double* lo, double* hi) {
+// Returns false for the boxes the family kernel never visits: end_3d skips the
+// whole r3 loop when the r3 range is empty (end_configuration.cu:225-227); the
+// subdivision of such a range can still produce a non-empty-looking box.
+__device__ __forceinline__ bool lattice_box(const LatticeSpec& s, const int* ix, double single, double* lo, double* hi) {
     const Iv la = subinterval(Iv{s.outer_lo, s.outer_hi}, ix[0], s.n[0]);
     const Iv r1 = subinterval(range_r1(la, single), ix[1], s.n[1]);
     const Iv r2 = subinterval(range_r2(s.fam, la, r1), ix[2], s.n[2]);
@@ -63,9 +66,12 @@ __device__ __forceinline__ void lattice_box(const LatticeSpec& s, const int* ix,
     lo[1] = r1.lo, hi[1] = r1.hi;
     lo[2] = r2.lo, hi[2] = r2.hi;
     if (family_dims(s.fam) == 4) {
-        const Iv r3 = subinterval(range_r3(s.fam, la, r2), ix[3], s.n[3]);
+        const Iv r3r = range_r3(s.fam, la, r2);
+        const Iv r3 = subinterval(r3r, ix[3], s.n[3]);
         lo[3] = r3.lo, hi[3] = r3.hi;
+        if (s.fam == F_END_3D && iempty(r3r)) return false;
     }
+    return true;
 }
 
 }  // namespace cpb

@@ -121,9 +121,11 @@ cp_status cp_eval_boxes_host(int family, int precision, int mode, const double* 
  * lambda, r1, r2[, r3], last fastest) the raw box the reference's kernel loop
  * builds with get_subinterval (subintervals.hpp:31-42) over its dependent
  * ranges (compute_r*_range, e.g. middle_configuration.cu:66-84).
- * sizes: subdivision count per axis (host array of dims entries). */
+ * sizes: subdivision count per axis (host array of dims entries).
+ * visited: NULL or n bytes, 0 where the kernel never visits the box (end_3d
+ * skips empty r3 ranges, end_configuration.cu:225-227). */
 cp_status cp_lattice_boxes(int family, double outer_lb, double outer_ub, const int32_t* sizes, const int64_t* index,
-                           size_t n, double* lo, double* hi, size_t stride, void* stream);
+                           size_t n, double* lo, double* hi, size_t stride, uint8_t* visited, void* stream);
 
 /* lower_bound_radius_single_placement(lb_lambda) for n values
  * (lower_bound_radius_single_placement.cu:26-61).  Device arrays. */
@@ -139,6 +141,133 @@ cp_status cp_eval_primitive(int kind, const double* args, size_t n, double* out,
 
 /* Diagnostics: outward-padded asin bounds (interval.cuh:420-438).  Device arrays. */
 cp_status cp_asin_pad(const double* x, size_t n, double* rd, double* ru, void* stream);
+
+
+/* ---------------------------------------------------------------- prover handle
+ * A handle owns device scratch (worklists, tables, counters) and a stream, so
+ * concurrent handles are independent; one handle must not be used from two
+ * threads at once.  cp_create makes `device` current for the calling thread. */
+typedef struct cp_prover cp_prover;
+
+cp_status cp_create(int device, cp_prover** out);
+void cp_destroy(cp_prover* p);
+
+/* The handle's CUDA stream (cudaStream_t as void*): every kernel the handle
+ * launches runs on it, so callers can record events around calls. */
+void* cp_get_stream(cp_prover* p);
+
+/* Requests that a running cp_prove_family_reference stop after its current
+ * launch (the reference's SIGINT handling, run_kernel.cuh:36-59).  Safe to call
+ * from a signal handler or another thread. */
+void cp_request_interrupt(cp_prover* p);
+
+/* Split policies for the box refinement. */
+typedef enum cp_split_policy {
+    CP_SPLIT_UNIFORM = 0, /* bisect every axis (2^dims children) */
+    CP_SPLIT_LAMBDA = 1,  /* bisect lambda only (the reference refines lambda only) */
+    CP_SPLIT_WIDEST = 2,  /* bisect the axis with the largest relative width */
+    CP_SPLIT_LEARNED = 3  /* bisect the axis the learned model picks (cp_load_model) */
+} cp_split_policy;
+
+typedef struct cp_refine_opts {
+    int32_t family;
+    int32_t precision;      /* cp_precision */
+    int32_t policy;         /* cp_split_policy */
+    int32_t max_depth;      /* a box not proved at this depth is unresolved (<= 250) */
+    int32_t seed_sizes[4];  /* lattice seed: subdivisions per axis */
+    double seed_lambda[2];  /* outer lambda interval of the lattice seed */
+    int64_t level_capacity; /* boxes per level buffer; 0 = 1<<25 */
+    int32_t block;          /* threads per block of the level kernel; 0 = 128 */
+    int32_t learned_order;  /* 1 = learned criterion order (needs cp_load_model) */
+} cp_refine_opts;
+
+typedef struct cp_refine_report {
+    int64_t evaluated;       /* boxes evaluated */
+    int64_t verdicts[5];     /* evaluated boxes per cp_verdict */
+    int64_t unresolved;      /* boxes not proved at max_depth */
+    int64_t clipped;         /* children outside the domain, dropped unevaluated */
+    int64_t fp32_decided;    /* boxes proved by the FP32 pass */
+    int64_t per_depth[64];   /* boxes evaluated per depth (depth >= 63 in the last) */
+    int32_t max_depth_seen;
+    int32_t launches;
+    double device_ms;        /* summed kernel time (CUDA events on the handle's stream) */
+    double wall_ms;          /* host wall time of the call */
+} cp_refine_report;
+
+/* Refines a family's lattice seed until every box is proved / empty or reaches
+ * max_depth.  The seed is the family lattice of opts->seed_sizes over
+ * opts->seed_lambda (the boxes cp_lattice_boxes returns); not-proved boxes are
+ * bisected per opts->policy and each child is clipped to the dependent ranges
+ * of its own lambda interval.  Synchronous.  Returns CP_OK when the search ran
+ * to completion (check report->unresolved), or an error status. */
+cp_status cp_refine(cp_prover* p, const cp_refine_opts* opts, cp_refine_report* report);
+
+/* As cp_refine from explicit device seed boxes (SoA with stride n, depth bytes
+ * may be NULL = 0). */
+cp_status cp_refine_boxes(cp_prover* p, const cp_refine_opts* opts, const double* lo, const double* hi,
+                          const uint8_t* depth, size_t n, cp_refine_report* report);
+
+/* ---------------------------------------------------------------- reference semantics
+ * One launch of a family kernel over one lambda interval with the reference's
+ * lattice sizes (run_kernel.cuh:81-84): the smallest lambda.lb of a lattice box
+ * whose guarded criteria fail, or +inf when none does (the reference returns
+ * DBL_MAX).  Lambda slabs are evaluated in increasing order and the search stops
+ * at the first slab holding a failing box.  sizes: NULL = the reference's sizes
+ * (start_configuration.cu:41-53, middle_configuration.cu:39-42,
+ * end_configuration.cu:39-49).  Returns CP_ERR_NOFIT / CP_ERR_TRAP_SITE where
+ * the reference kernel would trap (err_box: 8 doubles lo/hi of the box, or NULL). */
+cp_status cp_reference_step(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,
+                            double* first_critical, double* err_box);
+
+typedef struct cp_reference_report {
+    int32_t proved;          /* 1 when the lambda queue emptied */
+    int32_t interrupted;     /* 1 when stopped by cp_request_interrupt */
+    int64_t launches;        /* lattice launches (steps) */
+    int64_t boxes_evaluated; /* lattice boxes evaluated */
+    double remaining[2];     /* first remaining lambda interval when not proved */
+    double device_ms;
+    double wall_ms;
+} cp_reference_report;
+
+/* The reference's refinement loop run_kernel_until_no_criticals
+ * (run_kernel.cuh:61-132) over [la_lb, la_ub]: a min-queue of lambda intervals
+ * keyed on lb; each step is cp_reference_step; a failing interval continues on
+ * [first, ub] or splits at 0.5*(first+ub).  Stops after max_launches (0 = no
+ * limit) or on cp_request_interrupt.  trace: NULL or room for 3*max_launches
+ * doubles (lb, ub, first) per step. */
+cp_status cp_prove_family_reference(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,
+                                    int64_t max_launches, double* trace, cp_reference_report* report);
+
+/* Every failing box of one lattice launch (the reference's output_criticals
+ * rerun, run_kernel.cuh:86-108): up to max_boxes records of 8 doubles (lo/hi of
+ * la, r1, r2, r3 after tightening, host memory) plus one byte of failed handle
+ * bits each.  *count receives the number of failing boxes found. */
+cp_status cp_reference_criticals(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,
+                                 size_t max_boxes, double* boxes, uint8_t* handles, size_t* count);
+
+/* As cp_refine_boxes with HOST seed buffers (lo/hi SoA with stride n): copies
+ * the seeds into the handle's worklist, refines, synchronises. */
+cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* opts, const double* lo, const double* hi,
+                               const uint8_t* depth, size_t n, cp_refine_report* report);
+
+/* Diagnostics: measured peak throughput (operations per second, whole device)
+ * of the FP64 primitives the criteria use, each run alone with full occupancy
+ * and independent chains: rates[0] DFMA, [1] __dadd_rd, [2] __dmul_rd,
+ * [3] __ddiv_rd, [4] asin (CUDA libm), [5] FFMA (FP32).  Synchronous. */
+cp_status cp_measure_primitives(int device, double* rates);
+
+/* ---------------------------------------------------------------- autotuning
+ * The level kernel is compiled in CP_LEVEL_VARIANTS register/occupancy variants
+ * (minimum resident 128-thread blocks per SM 1, 4, 5, 6).  cp_autotune runs
+ * opts' refinement once per variant (after one warm-up run) and keeps the
+ * fastest for (opts->family, opts->precision) in the handle.  ms: NULL or
+ * CP_LEVEL_VARIANTS doubles receiving each variant's kernel time.  Returns the
+ * chosen variant in *best. */
+#define CP_LEVEL_VARIANTS 4
+cp_status cp_autotune(cp_prover* p, const cp_refine_opts* opts, int* best, double* ms);
+
+/* Selects a level-kernel variant explicitly (0 .. CP_LEVEL_VARIANTS-1). */
+cp_status cp_set_level_variant(cp_prover* p, int family, int precision, int variant);
 
 #ifdef __cplusplus
 }

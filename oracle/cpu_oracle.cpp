@@ -755,7 +755,9 @@ struct LatticeSpec {
     Iv outer;
     bool fused;
 };
-static void lattice_box(const LatticeSpec& s, const int* ix, double single, double* lo, double* hi) {
+// Returns false for boxes the kernel never visits: end_configuration.cu:225-227
+// skips the r3 loop when the r3 range is empty.
+static bool lattice_box(const LatticeSpec& s, const int* ix, double single, double* lo, double* hi) {
     Iv la = subinterval(s.outer, ix[0], s.n[0], s.fused);
     Iv r1 = subinterval(range_r1(la, single), ix[1], s.n[1], s.fused);
     Iv r2 = subinterval(range_r2(s.fam, la, r1), ix[2], s.n[2], s.fused);
@@ -763,9 +765,12 @@ static void lattice_box(const LatticeSpec& s, const int* ix, double single, doub
     lo[1] = r1.lb; hi[1] = r1.ub;
     lo[2] = r2.lb; hi[2] = r2.ub;
     if (family_dims(s.fam) == 4) {
-        Iv r3 = subinterval(range_r3(s.fam, la, r2), ix[3], s.n[3], s.fused);
+        Iv r3r = range_r3(s.fam, la, r2);
+        Iv r3 = subinterval(r3r, ix[3], s.n[3], s.fused);
         lo[3] = r3.lb; hi[3] = r3.ub;
+        if (s.fam == END_3D && iempty(r3r)) return false;
     }
+    return true;
 }
 static inline void unravel(const LatticeSpec& s, int64_t idx, int* ix) {
     int dims = family_dims(s.fam);
@@ -961,7 +966,10 @@ int orc_eval_lattice(int fam, double outer_lb, double outer_ub, const int32_t* s
         Out o;
         for (int64_t i = b; i < e; ++i) {
             unravel(s, i, ix);
-            lattice_box(s, ix, single[ix[0]], l, hh);
+            if (!lattice_box(s, ix, single[ix[0]], l, hh)) {
+                h[(size_t)t * 5 + V_EMPTY]++;
+                continue;
+            }
             eval_box(fam, l, hh, o);
             h[(size_t)t * 5 + o.verdict]++;
             if ((o.mask & 0x3F) && l[0] < fc[t]) fc[t] = l[0];

@@ -160,3 +160,29 @@ def test_host_entry_matches_device_entry(cp, oracle, family):
     v, m = cp.eval_boxes(family, lo, hi)
     hv, hm = cp.eval_boxes_host(family, lo, hi)
     assert (v.cpu().numpy() == hv).all() and (m.cpu().numpy() == hm).all()
+
+
+@pytest.mark.parametrize("family", range(6))
+def test_fp32_prepass_reproduces_fp64(cp, oracle, family):
+    """The FP32 certified shadow issues a verdict only when it equals the FP64
+    one: DECIDE verdict and mask per box, and the FULL-mode result."""
+    lo, hi = _mixed_boxes(oracle, family, seed=500 + family)
+    for mode in (cp.EVAL_DECIDE, cp.EVAL_FULL):
+        for order in (0, 1):
+            o = np.full(lo.shape[1], order, np.uint8)
+            v64, m64 = cp.eval_boxes(family, lo, hi, precision=cp.FP64, mode=mode, order=o)
+            v32, m32 = cp.eval_boxes(family, lo, hi, precision=cp.FP32_PREFILTER, mode=mode, order=o)
+            assert (v64.cpu().numpy() == v32.cpu().numpy()).all()
+            assert (m64.cpu().numpy() == m32.cpu().numpy()).all()
+
+
+@pytest.mark.parametrize("family", [0, 3, 5])
+def test_fp32_prepass_decides_most_fine_boxes(cp, oracle, family):
+    """On fine lattice boxes (mostly proved) the pre-pass settles most of them;
+    measured through the refinement report."""
+    dims = boxgen.DIMS[family]
+    p = cp.Prover(0)
+    r = p.refine(family, precision=cp.FP32_PREFILTER, max_depth=0, seed_sizes=[64, 32, 32, 8][:dims],
+                 seed_lambda=(0.6, 0.6005))
+    p.close()
+    assert r["fp32_decided"] >= 0.5 * r["evaluated"]
