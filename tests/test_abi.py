@@ -58,3 +58,16 @@ def test_invalid_arguments_rejected_without_device(libpath):
     assert L.cp_eval_boxes(7, 0, 0, None, None, 10, 10, None, None, None, None, None) == 1
     assert L.cp_eval_boxes(3, 5, 0, None, None, 10, 10, None, None, None, None, None) == 1
     assert L.cp_eval_boxes(3, 0, 0, None, None, 0, 0, None, None, None, None, None) == 0
+
+
+def test_reference_prover_links_against_shim(libpath, tmp_path):
+    """The reference's own prover.cpp links unchanged against the library (the
+    C++ shim defines circlepacking::lane_packing::find_critical_intervals)."""
+    ref = "/root/reference/code"
+    if not os.path.exists(os.path.join(ref, "prover.cpp")):
+        pytest.skip("reference sources not present on this machine")
+    out = tmp_path / "prover_b200"
+    libdir = os.path.dirname(libpath)
+    subprocess.run(["g++", "-std=c++17", f"-I{ref}/algcuda/cuda-cpp-wrapper/include", f"{ref}/prover.cpp",
+                    f"-L{libdir}", "-lcp_b200", f"-Wl,-rpath,{libdir}", "-o", str(out)], check=True)
+    assert out.exists()
