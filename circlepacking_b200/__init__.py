@@ -234,6 +234,7 @@ def _declare_handle(L):
     L.cp_get_stream.argtypes = [P]
     L.cp_get_stream.restype = P
     L.cp_autotune.argtypes = [P, ctypes.POINTER(RefineOpts), ctypes.POINTER(ctypes.c_int), P]
+    L.cp_refine_boxes_static.argtypes = [I, I, I, I, P, P, P, SZ, ctypes.POINTER(RefineReport), P]
     L.cp_set_level_variant.argtypes = [P, I, I, I]
 
 
@@ -364,3 +365,22 @@ class Prover:
                "cp_reference_criticals")
         m = min(count.value, max_boxes)
         return count.value, boxes[:m], handles[:m]
+
+
+STATIC_MAX_SEEDS, STATIC_MAX_DEPTH = 65536, 6
+
+
+def refine_boxes_static(family, lo, hi, depth=None, precision=FP64, policy=SPLIT_WIDEST, max_depth=6) -> dict:
+    """cp_refine_boxes_static: the refinement of explicit device seed boxes for
+    callers that cannot let the library allocate (all scratch lives in a fixed
+    array inside the library; see include/cp_prover.h)."""
+    torch = _torch()
+    L = lib()
+    _declare_handle(L)
+    lo = _dev(lo, torch.float64)
+    hi = _dev(hi, torch.float64)
+    dp = _dev(depth, torch.uint8) if depth is not None else None
+    r = RefineReport()
+    _check(L.cp_refine_boxes_static(family, precision, policy, max_depth, _ptr(lo), _ptr(hi), _ptr(dp), lo.shape[1],
+                                    ctypes.byref(r), _stream()), "cp_refine_boxes_static")
+    return r.as_dict()

@@ -1,6 +1,7 @@
 // Status strings and CUDA error bookkeeping of the C ABI.
 #include "cp_common.h"
 
+#include <cstdarg>
 #include <cstdio>
 #include <cstring>
 
@@ -10,6 +11,14 @@ thread_local char t_last_error[256] = "";
 
 cp_status cp_record_cuda_error(cudaError_t e, cp_status status) {
     std::snprintf(t_last_error, sizeof(t_last_error), "%s: %s", cudaGetErrorName(e), cudaGetErrorString(e));
+    return status;
+}
+
+cp_status cp_fail(cp_status status, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(t_last_error, sizeof(t_last_error), fmt, ap);
+    va_end(ap);
     return status;
 }
 

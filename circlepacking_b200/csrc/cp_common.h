@@ -14,6 +14,9 @@ constexpr int kEvalBlock = 128;
 // Records a CUDA error for cp_last_error_string() and returns `status`.
 cp_status cp_record_cuda_error(cudaError_t e, cp_status status);
 
+// Records a formatted message for cp_last_error_string() and returns `status`.
+cp_status cp_fail(cp_status status, const char* fmt, ...);
+
 // Checks for a launch error right after a kernel launch.
 cp_status cp_check_launch();
 

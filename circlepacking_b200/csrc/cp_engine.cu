@@ -416,6 +416,58 @@ void reference_sizes(int fam, int* n) {
 
 }  // namespace
 
+// ------------------------------------------------------------------ engine pieces
+size_t cp_engine_counter_words() { return (size_t)(C_COUNT + kDepthBins); }
+
+cp_status cp_engine_launch_table(double lambda_lo, double h, int n, double* t, double* v, cudaStream_t st) {
+    k_single_table<<<64, 128, 0, st>>>(lambda_lo, h, n, t, v);
+    return cp_check_launch();
+}
+
+cp_status cp_engine_launch_level(int fam, int prec, int variant, const BoxList& in, size_t begin, size_t count,
+                                 const BoxList* out, unsigned long long out_base, unsigned long long* counters,
+                                 const double* tab_t, const double* tab_v, int tab_n, double tab_h, int policy,
+                                 int max_depth, cudaStream_t st) {
+    LevelArgs a;
+    a.in = in;
+    a.begin = begin;
+    a.count = count;
+    a.out = out ? *out : BoxList{nullptr, nullptr, nullptr, 0};
+    a.cnt = counters;
+    a.per_depth = counters + C_COUNT;
+    a.tab = SingleTable{tab_t, tab_v, tab_n, tab_h};
+    a.policy = policy == CP_SPLIT_LEARNED ? SPLIT_GIVEN : policy;
+    a.max_depth = out ? max_depth : 0;
+    a.axis_hint = nullptr;
+    a.order_hint = nullptr;
+    cudaError_t e = cudaMemcpyAsync(counters + C_OUT, &out_base, sizeof(out_base), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cp_record_cuda_error(e, CP_ERR_CUDA);
+    LevelKernel k = level_kernel(fam, prec, variant);
+    const int block = kEvalBlock;
+    unsigned grid = grid_of(k, block);
+    const size_t need = (count + block - 1) / block;
+    if (need < grid) grid = (unsigned)std::max<size_t>(need, 1);
+    k<<<grid, block, 0, st>>>(a);
+    return cp_check_launch();
+}
+
+bool cp_engine_overflowed(const unsigned long long* h) { return (h[C_ERR] & E_OVERFLOW) != 0; }
+unsigned long long cp_engine_children(const unsigned long long* h) { return h[C_OUT]; }
+
+void cp_engine_fill_report(const unsigned long long* h, cp_refine_report* r) {
+    for (int v = 0; v < 5; ++v) r->verdicts[v] = (int64_t)h[C_VERDICT + v];
+    r->unresolved = (int64_t)h[C_UNRESOLVED];
+    r->clipped = (int64_t)h[C_CLIPPED];
+    r->fp32_decided = (int64_t)h[C_FP32];
+    r->evaluated = 0;
+    for (int v = 0; v < 5; ++v) r->evaluated += r->verdicts[v];
+    r->max_depth_seen = 0;
+    for (int d = 0; d < kDepthBins; ++d) {
+        r->per_depth[d] = (int64_t)h[C_COUNT + d];
+        if (r->per_depth[d]) r->max_depth_seen = d;
+    }
+}
+
 // ------------------------------------------------------------------ internal API
 cp_status cp_engine_eval_chunk(cp_prover* p, int fam, const cp_refine_opts& o, LevelBuf& in, size_t begin,
                                size_t count, LevelBuf* out, const uint8_t* axis_hint, const uint8_t* order_hint,

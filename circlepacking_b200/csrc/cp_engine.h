@@ -18,3 +18,16 @@ cp_status cp_model_hints(cp_prover* p, int fam, const cpb::BoxList& in, size_t b
                          uint8_t** order);
 // Releases the model state of a handle.
 void cp_model_free(cp_prover* p);
+
+// Pieces of the refinement engine reused by the static-scratch entry point
+// (cp_noalloc.cu).  Counters: cp_engine_counter_words() 64-bit words.
+size_t cp_engine_counter_words();
+cp_status cp_engine_launch_table(double lambda_lo, double h, int n, double* t, double* v, cudaStream_t st);
+cp_status cp_engine_launch_level(int fam, int prec, int variant, const cpb::BoxList& in, size_t begin, size_t count,
+                                 const cpb::BoxList* out, unsigned long long out_base, unsigned long long* counters,
+                                 const double* tab_t, const double* tab_v, int tab_n, double tab_h, int policy,
+                                 int max_depth, cudaStream_t st);
+// Reads the overflow flag and children count of a counter block copied to the host.
+bool cp_engine_overflowed(const unsigned long long* h_counters);
+unsigned long long cp_engine_children(const unsigned long long* h_counters);
+void cp_engine_fill_report(const unsigned long long* h_counters, cp_refine_report* r);

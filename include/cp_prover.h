@@ -269,6 +269,32 @@ cp_status cp_autotune(cp_prover* p, const cp_refine_opts* opts, int* best, doubl
 /* Selects a level-kernel variant explicitly (0 .. CP_LEVEL_VARIANTS-1). */
 cp_status cp_set_level_variant(cp_prover* p, int family, int precision, int variant);
 
+/* ---------------------------------------------------------------- no allocation
+ * This entry point has no counterpart in the reference.
+ *
+ * Box refinement for callers that cannot let a library allocate device memory:
+ * programs that route every device allocation through their own pool or
+ * caching allocator, and latency-critical loops where cudaMalloc's implicit
+ * device synchronisation is not acceptable.  It runs the same refinement as
+ * cp_refine_boxes (same verdicts, same report) but keeps all its scratch --
+ * counters, a single-placement table and the level buffers -- in one fixed
+ * 32 MiB array compiled into the library (held on every device that uses it
+ * until the process exits), and calls no cudaMalloc or cudaFree.
+ *   lo, hi, depth: device seed boxes (SoA, stride n; depth may be NULL = 0);
+ *   report: host memory, filled on return; the call synchronises `stream`.
+ * Limits: n <= CP_STATIC_MAX_SEEDS and max_depth <= CP_STATIC_MAX_DEPTH; larger
+ * requests return CP_ERR_CAPACITY (message in cp_last_error_string()).
+ * precision: cp_precision; policy: CP_SPLIT_UNIFORM, _LAMBDA or _WIDEST.
+ * The first call on each device sets the array up (resolves its address and
+ * fills the table with one kernel launch): make that call before any stream
+ * capture.  All calls on a device share the array: calls that overlap on the
+ * GPU race and must not be issued. */
+#define CP_STATIC_MAX_SEEDS 65536
+#define CP_STATIC_MAX_DEPTH 6
+cp_status cp_refine_boxes_static(int family, int precision, int policy, int max_depth, const double* lo,
+                                 const double* hi, const uint8_t* depth, size_t n, cp_refine_report* report,
+                                 void* stream);
+
 #ifdef __cplusplus
 }
 #endif
