@@ -30,6 +30,7 @@ UNIT = "boxes/s"
 FAMILIES = range(6)
 DIMS = (4, 3, 4, 4, 3, 4)
 SEED_RES = 64
+LEVEL_CAP = 1 << 25
 
 
 def parse():
@@ -44,6 +45,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--families", default="0,1,2,3,4,5", help="comma list (profiling runs)")
+    ap.add_argument("--seed-res", type=int, default=64, help="lattice subdivisions per axis of the seed")
+    ap.add_argument("--level-capacity", type=int, default=1 << 25, help="boxes per worklist level buffer")
+    ap.add_argument("--no-autotune", action="store_true", help="default kernel variants, FP64 (profiling runs)")
     return ap.parse_args()
 
 
@@ -150,7 +154,7 @@ def seed_opts(family, precision, depth):
 
     return dict(precision=precision, policy=cp.SPLIT_UNIFORM, max_depth=depth,
                 seed_sizes=[SEED_RES] * DIMS[family], seed_lambda=(cp.LAMBDA_MIN, cp.LAMBDA_MAX),
-                level_capacity=1 << 25)
+                level_capacity=LEVEL_CAP)
 
 
 def run_step(prover, precision, depth):
@@ -295,8 +299,9 @@ def main_reference(args, world, rank):
 
 def main():
     args = parse()
-    global FAMILIES
+    global FAMILIES, SEED_RES, LEVEL_CAP
     FAMILIES = [int(x) for x in args.families.split(",")]
+    SEED_RES, LEVEL_CAP = args.seed_res, args.level_capacity
     world, rank, local = dist_init()
     if args.impl == "reference":
         main_reference(args, world, rank)
@@ -311,7 +316,11 @@ def main():
     FP64, PRE = cp.FP64, cp.FP32_PREFILTER
 
     # ---- autotune (outside the timed region): kernel variant and precision per family
-    chosen, tuning = autotune(prover, cp)
+    if args.no_autotune:
+        chosen = {f: FP64 for f in FAMILIES}
+        tuning = {cp.FAMILIES[f]: {"precision": "fp64", "variant": 0} for f in FAMILIES}
+    else:
+        chosen, tuning = autotune(prover, cp)
 
     def use_plain(on):
         # the plain arm: FP64 with the untuned default kernel variant

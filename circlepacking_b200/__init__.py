@@ -197,13 +197,13 @@ class RefineReport(ctypes.Structure):
     _fields_ = [("evaluated", ctypes.c_int64), ("verdicts", ctypes.c_int64 * 5), ("unresolved", ctypes.c_int64),
                 ("clipped", ctypes.c_int64), ("fp32_decided", ctypes.c_int64), ("per_depth", ctypes.c_int64 * 64),
                 ("max_depth_seen", ctypes.c_int32), ("launches", ctypes.c_int32), ("device_ms", ctypes.c_double),
-                ("wall_ms", ctypes.c_double)]
+                ("wall_ms", ctypes.c_double), ("handles_evaluated", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         return dict(evaluated=self.evaluated, verdicts=list(self.verdicts), unresolved=self.unresolved,
                     clipped=self.clipped, fp32_decided=self.fp32_decided,
                     per_depth=list(self.per_depth)[: self.max_depth_seen + 1], launches=self.launches,
-                    device_ms=self.device_ms, wall_ms=self.wall_ms)
+                    device_ms=self.device_ms, wall_ms=self.wall_ms, handles_evaluated=self.handles_evaluated)
 
 
 class ReferenceReport(ctypes.Structure):

@@ -35,6 +35,7 @@ enum : int {
     C_COLLECT = 22,
     C_NOFIT_SLAB = 23,  // smallest lambda slab holding a box whose fit check fired (middle/end)
     C_TRAP_SLAB = 24,   // smallest lambda slab holding a box that reached a trap site
+    C_HANDLES = 25,     // guarded criteria evaluated in FP64
     C_COUNT = 26
 };
 enum : unsigned long long { E_OVERFLOW = 1, E_NOFIT = 2, E_TRAP = 4 };
@@ -75,9 +76,12 @@ __global__ void __launch_bounds__(kEvalBlock, MINB) k_level(LevelArgs a) {
     constexpr int D = family_dims(FAM);
     __shared__ unsigned long long s_hist[8];
     __shared__ unsigned long long s_depth[kDepthBins];
+    __shared__ unsigned long long s_handles;
     for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x) s_depth[t] = 0;
     if (threadIdx.x < 8) s_hist[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s_handles = 0;
     __syncthreads();
+    unsigned handles = 0;
     const size_t step = (size_t)gridDim.x * blockDim.x;
     for (size_t base = (size_t)blockIdx.x * blockDim.x; base < a.count; base += step) {
         const size_t j = base + threadIdx.x;
@@ -101,13 +105,17 @@ __global__ void __launch_bounds__(kEvalBlock, MINB) k_level(LevelArgs a) {
                     uint8_t pmask;
                     const int pre = prefilter_box<FAM>(lo, hi, ord, false, &pmask);
                     if (pre == PF_UNDECIDED) {
-                        v = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr).verdict;
+                        const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr);
+                        v = r.verdict;
+                        handles += r.handles;
                     } else {
                         v = pre == PF_PROVED ? V_PROVED : pre == PF_EMPTY ? V_EMPTY : pre == PF_NOFIT ? V_NOFIT : V_CRITICAL;
                         if (pre != PF_EMPTY) atomicAdd(&s_hist[C_FP32], 1ull);
                     }
                 } else {
-                    v = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr).verdict;
+                    const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr);
+                    v = r.verdict;
+                    handles += r.handles;
                 }
                 atomicAdd(&s_hist[v], 1ull);
                 atomicAdd(&s_depth[depth < kDepthBins ? depth : kDepthBins - 1], 1ull);
@@ -144,9 +152,13 @@ __global__ void __launch_bounds__(kEvalBlock, MINB) k_level(LevelArgs a) {
             }
         }
     }
+    // one shared-memory add per warp for the handle count
+    for (int off = 16; off > 0; off >>= 1) handles += __shfl_xor_sync(0xffffffffu, handles, off);
+    if ((threadIdx.x & 31) == 0 && handles) atomicAdd(&s_handles, (unsigned long long)handles);
     __syncthreads();
     if (threadIdx.x < 8 && threadIdx.x != C_OUT && s_hist[threadIdx.x])
         atomicAdd(&a.cnt[threadIdx.x], s_hist[threadIdx.x]);
+    if (threadIdx.x == 0 && s_handles) atomicAdd(&a.cnt[C_HANDLES], s_handles);
     for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x)
         if (s_depth[t]) atomicAdd(&a.per_depth[t], s_depth[t]);
 }
@@ -459,6 +471,7 @@ void cp_engine_fill_report(const unsigned long long* h, cp_refine_report* r) {
     r->unresolved = (int64_t)h[C_UNRESOLVED];
     r->clipped = (int64_t)h[C_CLIPPED];
     r->fp32_decided = (int64_t)h[C_FP32];
+    r->handles_evaluated = (int64_t)h[C_HANDLES];
     r->evaluated = 0;
     for (int v = 0; v < 5; ++v) r->evaluated += r->verdicts[v];
     r->max_depth_seen = 0;
@@ -553,6 +566,7 @@ cp_status refine_levels(cp_prover* p, const cp_refine_opts& o, cp_refine_report*
     r->unresolved = (int64_t)p->h_cnt[C_UNRESOLVED];
     r->clipped = (int64_t)p->h_cnt[C_CLIPPED];
     r->fp32_decided = (int64_t)p->h_cnt[C_FP32];
+    r->handles_evaluated = (int64_t)p->h_cnt[C_HANDLES];
     r->evaluated = 0;
     for (int v = 0; v < 5; ++v) r->evaluated += r->verdicts[v];
     r->max_depth_seen = 0;

@@ -25,6 +25,7 @@ namespace cpb {
 
 struct Verdict {
     uint8_t verdict, mask;
+    uint8_t handles;  // guarded criteria (handles) evaluated for this box
 };
 
 enum EvalMode { FULL = 0, DECIDE = 1 };
@@ -201,6 +202,7 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
     if (iempty(la) || iempty(r1) || iempty(r2) || (D == 4 && iempty(r3))) return {V_EMPTY, 0};
 
     uint8_t mask = 0;
+    uint8_t handles = 0;
     bool trap = false;
     // the start+end kernels have no fit check (start_configuration.cu:190-215, 267-298)
     const bool fit_fires = FAM != F_START_END_2D && FAM != F_START_END_3D &&
@@ -221,6 +223,7 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
         const double ar1 = disk_area_lb(r1), ar2 = disk_area_lb(r2);
         const double so_hi = semi_outer_hi(r1);
         if (case1.pos) {
+            ++handles;
             double used = used_ub(ratio, __dadd_ru(so_hi, a12.hi));
             lhs = __dadd_rd(ar1, __dmul_rd(0.5, ar2));
             rhs = __dmul_ru(kCriticalRatio, used);
@@ -231,6 +234,7 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
             }
         }
         if (!case1.def) {
+            ++handles;
             double used = used_ub(ratio, __dadd_ru(so_hi, a13.hi));
             double ar3 = disk_area_lb(r3);
             lhs = __dadd_rd(__dadd_rd(ar1, ar2), __dmul_rd(0.5, ar3));
@@ -239,6 +243,7 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
             if (!(lhs >= rhs)) mask |= 2;
         }
     } else if (FAM == F_START_END_2D) {
+        handles = 1;
         const double a1_hi = semi_outer_hi(r1);
         const Iv a2{semi_inner_lo(la, r2), semi_inner_hi(la, r2)};
         const Iv a12 = ca_outer_inner(la, r1, r2, trap);
@@ -256,6 +261,7 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
         if (MODE == FULL) trace_put(tr, 0, lhs, rhs);
         if (!(lhs >= rhs)) mask |= 1;
     } else if (FAM == F_START_END_3D) {
+        handles = 1;
         const Iv a1{semi_outer_lo(r1), semi_outer_hi(r1)};
         const Iv a2{semi_inner_lo(la, r2), semi_inner_hi(la, r2)};
         const Iv a3{semi_outer_lo(r3), semi_outer_hi(r3)};
@@ -285,6 +291,7 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
         const bool second_first = (MODE == DECIDE) && (order & 1);
         for (int h = 0; h < 2; ++h) {
             const bool inner = (h == 0) != second_first;
+            ++handles;
             bool failed = middle_handle<MODE>(la, r1, r2, r3, inner, mask, inner ? 0 : 2, trap, tr);
             if (MODE == DECIDE && failed) break;
         }
@@ -292,6 +299,7 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
         const bool second_first = (MODE == DECIDE) && (order & 1);
         for (int h = 0; h < 2; ++h) {
             const bool inner = (h == 0) != second_first;
+            ++handles;
             bool failed = inner ? end2d_handle<true>(la, r1, r2, trap, &lhs, &rhs)
                                 : end2d_handle<false>(la, r1, r2, trap, &lhs, &rhs);
             const int k = inner ? 0 : 1;
@@ -305,6 +313,7 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
         const bool second_first = (MODE == DECIDE) && (order & 1);
         for (int h = 0; h < 2; ++h) {
             const bool inner = (h == 0) != second_first;
+            ++handles;
             bool evaluated = false;
             bool failed = inner ? end3d_handle<true>(la, r1, r2, r3, trap, &evaluated, &lhs, &rhs)
                                 : end3d_handle<false>(la, r1, r2, r3, trap, &evaluated, &lhs, &rhs);
@@ -327,7 +336,7 @@ done:
         v = V_CRITICAL;
     else
         v = V_PROVED;
-    return {v, mask};
+    return {v, mask, handles};
 }
 
 }  // namespace cpb

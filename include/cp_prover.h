@@ -192,6 +192,7 @@ typedef struct cp_refine_report {
     int32_t launches;
     double device_ms;        /* summed kernel time (CUDA events on the handle's stream) */
     double wall_ms;          /* host wall time of the call */
+    int64_t handles_evaluated; /* guarded criteria evaluated in FP64 (DECIDE order) */
 } cp_refine_report;
 
 /* Refines a family's lattice seed until every box is proved / empty or reaches
