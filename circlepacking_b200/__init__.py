@@ -384,3 +384,92 @@ def refine_boxes_static(family, lo, hi, depth=None, precision=FP64, policy=SPLIT
     _check(L.cp_refine_boxes_static(family, precision, policy, max_depth, _ptr(lo), _ptr(hi), _ptr(dp), lo.shape[1],
                                     ctypes.byref(r), _stream()), "cp_refine_boxes_static")
     return r.as_dict()
+
+
+# ---------------------------------------------------------------- learned proposal model
+def _declare_model(L):
+    P, I, SZ, I64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_int64
+    L.cp_model_collect.argtypes = [P, ctypes.POINTER(RefineOpts), I64, ctypes.c_int32, ctypes.POINTER(I64)]
+    L.cp_model_records.argtypes = [P, P, P, P, P, P, SZ, ctypes.POINTER(SZ)]
+    L.cp_model_train.argtypes = [P, I, I, I, ctypes.c_float, ctypes.c_uint64, P]
+    L.cp_model_get_params.argtypes = [P, I, P]
+    L.cp_model_set_params.argtypes = [P, I, P]
+    L.cp_model_loss_grad.argtypes = [I, P, P, P, P, SZ, P, P]
+    L.cp_model_predict.argtypes = [P, I, P, P, P, SZ, P, P, P]
+
+
+def model_param_count() -> int:
+    return int(lib().cp_model_param_count())
+
+
+def model_loss_grad(family, params, feats, crit, axis):
+    """One GPU forward+backward pass (no optimiser step): (loss, grad)."""
+    L = lib()
+    _declare_model(L)
+    params = np.ascontiguousarray(params, np.float32)
+    feats = np.ascontiguousarray(feats, np.float32)
+    crit = np.ascontiguousarray(crit, np.uint8)
+    axis = np.ascontiguousarray(axis, np.int8)
+    loss = np.zeros(1, np.float32)
+    grad = np.zeros(params.size, np.float32)
+    _check(L.cp_model_loss_grad(family, params.ctypes.data, feats.ctypes.data, crit.ctypes.data, axis.ctypes.data,
+                                feats.shape[0], loss.ctypes.data, grad.ctypes.data), "cp_model_loss_grad")
+    return float(loss[0]), grad
+
+
+class _ModelMixin:
+    def model_collect(self, family, max_records, sample_stride=1, **kw) -> int:
+        _declare_model(self._L)
+        o = self.opts(family, **kw)
+        n = ctypes.c_int64()
+        _check(self._L.cp_model_collect(self._h, ctypes.byref(o), max_records, sample_stride, ctypes.byref(n)),
+               "cp_model_collect")
+        return n.value
+
+    def model_records(self, cap=None) -> dict:
+        _declare_model(self._L)
+        n = ctypes.c_size_t()
+        _check(self._L.cp_model_records(self._h, None, None, None, None, None, 0, ctypes.byref(n)), "cp_model_records")
+        k = n.value if cap is None else min(cap, n.value)
+        feats = np.zeros((max(k, 1), 16), np.float32)
+        crit = np.zeros(max(k, 1), np.uint8)
+        axis = np.zeros(max(k, 1), np.int8)
+        boxes = np.zeros((max(k, 1), 8), np.float64)
+        depth = np.zeros(max(k, 1), np.uint8)
+        _check(self._L.cp_model_records(self._h, feats.ctypes.data, crit.ctypes.data, axis.ctypes.data,
+                                        boxes.ctypes.data, depth.ctypes.data, k, ctypes.byref(n)), "cp_model_records")
+        return dict(feats=feats[:k], crit=crit[:k], axis=axis[:k], boxes=boxes[:k], depth=depth[:k])
+
+    def model_train(self, family, epochs=20, batch=4096, lr=1e-3, seed=1):
+        _declare_model(self._L)
+        losses = np.zeros(epochs, np.float32)
+        _check(self._L.cp_model_train(self._h, family, epochs, batch, lr, seed, losses.ctypes.data), "cp_model_train")
+        return losses
+
+    def model_params(self, family):
+        _declare_model(self._L)
+        p = np.zeros(model_param_count(), np.float32)
+        _check(self._L.cp_model_get_params(self._h, family, p.ctypes.data), "cp_model_get_params")
+        return p
+
+    def model_set_params(self, family, params):
+        _declare_model(self._L)
+        p = np.ascontiguousarray(params, np.float32)
+        _check(self._L.cp_model_set_params(self._h, family, p.ctypes.data), "cp_model_set_params")
+
+    def model_predict(self, family, lo, hi, depth=None):
+        _declare_model(self._L)
+        lo = np.ascontiguousarray(lo, np.float64)
+        hi = np.ascontiguousarray(hi, np.float64)
+        n = lo.shape[1]
+        dp = np.ascontiguousarray(depth, np.uint8).ctypes.data if depth is not None else None
+        logits = np.zeros((n, 8), np.float32)
+        axis = np.zeros(n, np.uint8)
+        order = np.zeros(n, np.uint8)
+        _check(self._L.cp_model_predict(self._h, family, lo.ctypes.data, hi.ctypes.data, dp, n, logits.ctypes.data,
+                                        axis.ctypes.data, order.ctypes.data), "cp_model_predict")
+        return logits, axis, order
+
+
+for _name in ("model_collect", "model_records", "model_train", "model_params", "model_set_params", "model_predict"):
+    setattr(Prover, _name, getattr(_ModelMixin, _name))

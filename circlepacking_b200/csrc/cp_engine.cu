@@ -12,34 +12,11 @@
 
 #include "cp_common.h"
 #include "cp_engine.h"
-#include "cp_fp32.cuh"
-#include "cp_worklist.cuh"
+#include "cp_level.cuh"
 
 using namespace cpb;
 
 namespace {
-
-// counter block layout (unsigned long long)
-enum : int {
-    C_VERDICT = 0,  // 5 verdict counts
-    C_UNRESOLVED = 5,
-    C_CLIPPED = 6,
-    C_FP32 = 7,
-    C_OUT = 8,      // children appended
-    C_ERR = 9,      // error flags
-    C_BEST_SLAB = 10,
-    C_EVALUATED = 11,
-    C_FIRST_BITS = 12,  // ordered encoding of the smallest failing lambda.lb
-    C_ERRBOX_CLAIM = 13,
-    C_ERRBOX = 14,      // 8 slots: lo/hi of the first erroneous box
-    C_COLLECT = 22,
-    C_NOFIT_SLAB = 23,  // smallest lambda slab holding a box whose fit check fired (middle/end)
-    C_TRAP_SLAB = 24,   // smallest lambda slab holding a box that reached a trap site
-    C_HANDLES = 25,     // guarded criteria evaluated in FP64
-    C_COUNT = 26
-};
-enum : unsigned long long { E_OVERFLOW = 1, E_NOFIT = 2, E_TRAP = 4 };
-constexpr int kDepthBins = 64;
 
 // order-preserving map of a double onto unsigned 64-bit (the encoding of
 // Atomic_ordered_double, atomic_float.hpp:56-66)
@@ -57,110 +34,18 @@ __host__ __device__ __forceinline__ double ordered_value(unsigned long long u) {
     return v;
 }
 
-struct LevelArgs {
-    BoxList in;
-    size_t begin, count;
-    BoxList out;
-    unsigned long long* cnt;
-    unsigned long long* per_depth;
-    SingleTable tab;
-    int policy, max_depth;
-    const uint8_t* axis_hint;   // per input box (SPLIT_GIVEN), indexed from `begin`
-    const uint8_t* order_hint;  // per input box criterion order, or null
-};
-
 // MINB: minimum resident blocks per SM requested from the compiler (register cap
 // 65536 / (128 * MINB)); the autotuner picks the variant per family and precision.
 template <int FAM, int PREC, int MINB>
 __global__ void __launch_bounds__(kEvalBlock, MINB) k_level(LevelArgs a) {
-    constexpr int D = family_dims(FAM);
-    __shared__ unsigned long long s_hist[8];
-    __shared__ unsigned long long s_depth[kDepthBins];
-    __shared__ unsigned long long s_handles;
-    for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x) s_depth[t] = 0;
-    if (threadIdx.x < 8) s_hist[threadIdx.x] = 0;
-    if (threadIdx.x == 0) s_handles = 0;
+    __shared__ LevelSmem<kEvalBlock / 32> sm;
+    level_smem_init(sm);
     __syncthreads();
     unsigned handles = 0;
     const size_t step = (size_t)gridDim.x * blockDim.x;
-    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < a.count; base += step) {
-        const size_t j = base + threadIdx.x;
-        const size_t i = a.begin + j;
-        unsigned nchild = 0;
-        double lo[4], hi[4];
-        int depth = 0, axis = 0;
-        if (j < a.count) {
-            depth = a.in.depth[i];
-            if (depth == 0xFF) {
-                atomicAdd(&s_hist[C_CLIPPED], 1ull);
-            } else {
-#pragma unroll
-                for (int d = 0; d < D; ++d) {
-                    lo[d] = a.in.lo[d * a.in.cap + i];
-                    hi[d] = a.in.hi[d * a.in.cap + i];
-                }
-                const int ord = a.order_hint ? a.order_hint[j] : 0;
-                int v;
-                if (PREC == CP_FP32_PREFILTER) {
-                    uint8_t pmask;
-                    const int pre = prefilter_box<FAM>(lo, hi, ord, false, &pmask);
-                    if (pre == PF_UNDECIDED) {
-                        const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr);
-                        v = r.verdict;
-                        handles += r.handles;
-                    } else {
-                        v = pre == PF_PROVED ? V_PROVED : pre == PF_EMPTY ? V_EMPTY : pre == PF_NOFIT ? V_NOFIT : V_CRITICAL;
-                        if (pre != PF_EMPTY) atomicAdd(&s_hist[C_FP32], 1ull);
-                    }
-                } else {
-                    const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr);
-                    v = r.verdict;
-                    handles += r.handles;
-                }
-                atomicAdd(&s_hist[v], 1ull);
-                atomicAdd(&s_depth[depth < kDepthBins ? depth : kDepthBins - 1], 1ull);
-                if (v != V_PROVED && v != V_EMPTY) {
-                    if (depth >= a.max_depth) {
-                        atomicAdd(&s_hist[C_UNRESOLVED], 1ull);
-                    } else {
-                        nchild = fanout(a.policy, D);
-                        if (a.policy == SPLIT_WIDEST)
-                            axis = widest_axis<D>(lo, hi);
-                        else if (a.policy == SPLIT_GIVEN)
-                            axis = a.axis_hint ? (a.axis_hint[j] % D) : 0;
-                    }
-                }
-            }
-        }
-        const unsigned long long slot = warp_reserve(&a.cnt[C_OUT], nchild);
-        if (nchild) {
-            if (slot + nchild > a.out.cap) {
-                atomicOr(&a.cnt[C_ERR], E_OVERFLOW);
-            } else {
-                for (unsigned c = 0; c < nchild; ++c) {
-                    double clo[4], chi[4];
-                    make_child<D>(lo, hi, a.policy, axis, (int)c, clo, chi);
-                    const bool alive = clip_child<FAM>(clo, chi, a.tab);
-                    const size_t o = (size_t)(slot + c);
-#pragma unroll
-                    for (int d = 0; d < D; ++d) {
-                        a.out.lo[d * a.out.cap + o] = clo[d];
-                        a.out.hi[d * a.out.cap + o] = chi[d];
-                    }
-                    a.out.depth[o] = alive ? (uint8_t)(depth + 1) : (uint8_t)0xFF;
-                }
-            }
-        }
-    }
-    // one shared-memory add per warp for the handle count
-    for (int off = 16; off > 0; off >>= 1) handles += __shfl_xor_sync(0xffffffffu, handles, off);
-    if ((threadIdx.x & 31) == 0 && handles) atomicAdd(&s_handles, (unsigned long long)handles);
-    __syncthreads();
-    if (threadIdx.x < 8 && threadIdx.x != C_OUT && s_hist[threadIdx.x])
-        atomicAdd(&a.cnt[threadIdx.x], s_hist[threadIdx.x]);
-    if (threadIdx.x == 0 && s_handles) atomicAdd(&a.cnt[C_HANDLES], s_handles);
-    for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x)
-        if (s_depth[t]) atomicAdd(&a.per_depth[t], s_depth[t]);
+    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < a.count; base += step)
+        level_step<FAM, PREC>(a, base + threadIdx.x, sm, handles);
+    level_flush(a, sm, handles);
 }
 
 // Seed: every box of a family lattice, depth 0.
@@ -547,6 +432,8 @@ cp_status refine_levels(cp_prover* p, const cp_refine_opts& o, cp_refine_report*
         }
         const size_t begin = in.n - c;
         uint8_t *axis = nullptr, *order = nullptr;
+        if (cp_model_collecting(p))
+            CP_TRY(cp_model_collect_chunk(p, fam, in.b, begin, c, p->tab_t, p->tab_v, p->tab_n, p->tab_h));
         if (o.policy == CP_SPLIT_LEARNED || o.learned_order) {
             CP_TRY(cp_model_hints(p, fam, in.b, begin, c, o.policy == CP_SPLIT_LEARNED ? &axis : nullptr,
                                   o.learned_order ? &order : nullptr));

@@ -18,6 +18,11 @@ cp_status cp_model_hints(cp_prover* p, int fam, const cpb::BoxList& in, size_t b
                          uint8_t** order);
 // Releases the model state of a handle.
 void cp_model_free(cp_prover* p);
+// Trace recording (cp_model_collect): labels a sample of the chunk's boxes
+// before the engine evaluates it; a no-op unless a collection is running.
+bool cp_model_collecting(cp_prover* p);
+cp_status cp_model_collect_chunk(cp_prover* p, int fam, const cpb::BoxList& in, size_t begin, size_t count,
+                                 const double* tab_t, const double* tab_v, int tab_n, double tab_h);
 
 // Pieces of the refinement engine reused by the static-scratch entry point
 // (cp_noalloc.cu).  Counters: cp_engine_counter_words() 64-bit words.

@@ -1,0 +1,181 @@
+// The level step of the box refinement, shared by the level-synchronous
+// kernel (cp_engine.cu) and the persistent graph-driven kernel (cp_graph.cu):
+// evaluate one box per lane (DECIDE mode, optional FP32 pre-pass and per-box
+// criterion order), count verdicts, and append the children of every box that
+// is not proved to the next worklist level.
+#pragma once
+#include <cstdint>
+
+#include "cp_fp32.cuh"
+#include "cp_worklist.cuh"
+
+namespace cpb {
+
+// counter block layout (unsigned long long)
+enum : int {
+    C_VERDICT = 0,  // 5 verdict counts
+    C_UNRESOLVED = 5,
+    C_CLIPPED = 6,
+    C_FP32 = 7,
+    C_OUT = 8,      // children appended
+    C_ERR = 9,      // error flags
+    C_BEST_SLAB = 10,
+    C_EVALUATED = 11,
+    C_FIRST_BITS = 12,  // ordered encoding of the smallest failing lambda.lb
+    C_ERRBOX_CLAIM = 13,
+    C_ERRBOX = 14,      // 8 slots: lo/hi of the first erroneous box
+    C_COLLECT = 22,
+    C_NOFIT_SLAB = 23,  // smallest lambda slab holding a box whose fit check fired (middle/end)
+    C_TRAP_SLAB = 24,   // smallest lambda slab holding a box that reached a trap site
+    C_HANDLES = 25,     // guarded criteria evaluated in FP64
+    C_COUNT = 26
+};
+enum : unsigned long long { E_OVERFLOW = 1, E_NOFIT = 2, E_TRAP = 4 };
+constexpr int kDepthBins = 64;
+
+struct LevelArgs {
+    BoxList in;
+    size_t begin, count;
+    BoxList out;
+    unsigned long long* cnt;
+    unsigned long long* per_depth;
+    SingleTable tab;
+    int policy, max_depth;
+    const uint8_t* axis_hint;   // per input box (SPLIT_GIVEN), indexed from `begin`
+    const uint8_t* order_hint;  // per input box criterion order, or null
+};
+
+// Per-block shared state of the level step; WARPS = warps per block.
+template <int WARPS>
+struct LevelSmem {
+    unsigned long long hist[8];
+    unsigned long long depth[kDepthBins];
+    unsigned long long handles;
+    // per-warp staging of the parents of one iteration's children
+    struct Parent {
+        double lo[4], hi[4];
+    } par[WARPS][32];
+    uint16_t excl[WARPS][32];
+    uint8_t axis[WARPS][32], dep[WARPS][32];
+    uint8_t own[WARPS][32 * 16];
+};
+
+template <int WARPS>
+__device__ __forceinline__ void level_smem_init(LevelSmem<WARPS>& sm) {
+    for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x) sm.depth[t] = 0;
+    if (threadIdx.x < 8) sm.hist[threadIdx.x] = 0;
+    if (threadIdx.x == 0) sm.handles = 0;
+}
+
+// One lane's box j of the chunk (j >= a.count: the lane only takes part in the
+// warp's collective child write).  All 32 lanes of the warp must call it.
+template <int FAM, int PREC, int WARPS>
+__device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSmem<WARPS>& sm, unsigned& handles) {
+    constexpr int D = family_dims(FAM);
+    const size_t i = a.begin + j;
+    unsigned nchild = 0;
+    double lo[4], hi[4];
+    int depth = 0, axis = 0;
+    if (j < a.count) {
+        depth = a.in.depth[i];
+        if (depth == 0xFF) {
+            atomicAdd(&sm.hist[C_CLIPPED], 1ull);
+        } else {
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                lo[d] = a.in.lo[d * a.in.cap + i];
+                hi[d] = a.in.hi[d * a.in.cap + i];
+            }
+            const int ord = a.order_hint ? a.order_hint[j] : 0;
+            int v;
+            if (PREC == CP_FP32_PREFILTER) {
+                uint8_t pmask;
+                const int pre = prefilter_box<FAM>(lo, hi, ord, false, &pmask);
+                if (pre == PF_UNDECIDED) {
+                    const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr);
+                    v = r.verdict;
+                    handles += r.handles;
+                } else {
+                    v = pre == PF_PROVED ? V_PROVED : pre == PF_EMPTY ? V_EMPTY : pre == PF_NOFIT ? V_NOFIT : V_CRITICAL;
+                    if (pre != PF_EMPTY) atomicAdd(&sm.hist[C_FP32], 1ull);
+                }
+            } else {
+                const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr);
+                v = r.verdict;
+                handles += r.handles;
+            }
+            atomicAdd(&sm.hist[v], 1ull);
+            atomicAdd(&sm.depth[depth < kDepthBins ? depth : kDepthBins - 1], 1ull);
+            if (v != V_PROVED && v != V_EMPTY) {
+                if (depth >= a.max_depth) {
+                    atomicAdd(&sm.hist[C_UNRESOLVED], 1ull);
+                } else {
+                    nchild = fanout(a.policy, D);
+                    if (a.policy == SPLIT_WIDEST)
+                        axis = widest_axis<D>(lo, hi);
+                    else if (a.policy == SPLIT_GIVEN)
+                        axis = a.axis_hint ? (a.axis_hint[j] % D) : 0;
+                }
+            }
+        }
+    }
+    // children: the warp reserves one contiguous range and writes it
+    // cooperatively, lane k of an iteration writing slot k, so every store
+    // of an axis array is one coalesced 256-byte segment per warp
+    unsigned excl, total;
+    const unsigned long long wbase = warp_reserve_range(&a.cnt[C_OUT], nchild, &excl, &total);
+    if (total) {
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (wbase + total > a.out.cap) {
+            if (lane == 0) atomicOr(&a.cnt[C_ERR], E_OVERFLOW);
+        } else {
+            if (nchild) {
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    sm.par[w][lane].lo[d] = lo[d];
+                    sm.par[w][lane].hi[d] = hi[d];
+                }
+                sm.excl[w][lane] = (uint16_t)excl;
+                sm.axis[w][lane] = (uint8_t)axis;
+                sm.dep[w][lane] = (uint8_t)depth;
+                for (unsigned c = 0; c < nchild; ++c) sm.own[w][excl + c] = (uint8_t)lane;
+            }
+            __syncwarp();
+            for (unsigned k = lane; k < total; k += 32) {
+                const int own = sm.own[w][k];
+                const int c = (int)k - (int)sm.excl[w][own];
+                double plo[4], phi[4], clo[4], chi[4];
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    plo[d] = sm.par[w][own].lo[d];
+                    phi[d] = sm.par[w][own].hi[d];
+                }
+                make_child<D>(plo, phi, a.policy, sm.axis[w][own], c, clo, chi);
+                const bool alive = clip_child<FAM>(clo, chi, a.tab);
+                const size_t o = (size_t)(wbase + k);
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    a.out.lo[d * a.out.cap + o] = clo[d];
+                    a.out.hi[d * a.out.cap + o] = chi[d];
+                }
+                a.out.depth[o] = alive ? (uint8_t)(sm.dep[w][own] + 1) : (uint8_t)0xFF;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Adds the block's counts to the global counters (after the last step).
+template <int WARPS>
+__device__ __forceinline__ void level_flush(const LevelArgs& a, LevelSmem<WARPS>& sm, unsigned handles) {
+    for (int off = 16; off > 0; off >>= 1) handles += __shfl_xor_sync(0xffffffffu, handles, off);
+    if ((threadIdx.x & 31) == 0 && handles) atomicAdd(&sm.handles, (unsigned long long)handles);
+    __syncthreads();
+    if (threadIdx.x < 8 && threadIdx.x != C_OUT && sm.hist[threadIdx.x])
+        atomicAdd(&a.cnt[threadIdx.x], sm.hist[threadIdx.x]);
+    if (threadIdx.x == 0 && sm.handles) atomicAdd(&a.cnt[C_HANDLES], sm.handles);
+    for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x)
+        if (sm.depth[t]) atomicAdd(&a.per_depth[t], sm.depth[t]);
+}
+
+}  // namespace cpb

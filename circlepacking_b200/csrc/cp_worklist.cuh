@@ -132,4 +132,23 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned long long* c
     return base + (incl - count);
 }
 
+// As warp_reserve, for writers that emit the warp's slots cooperatively:
+// returns the warp's first slot; *excl = this lane's offset in the warp's range,
+// *total = the warp's slot count (uniform).  All lanes of the warp take part.
+__device__ __forceinline__ unsigned long long warp_reserve_range(unsigned long long* counter, unsigned count,
+                                                                 unsigned* excl, unsigned* total) {
+    const unsigned lane = threadIdx.x & 31;
+    unsigned incl = count;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        unsigned v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= (unsigned)off) incl += v;
+    }
+    *total = __shfl_sync(0xffffffffu, incl, 31);
+    *excl = incl - count;
+    unsigned long long base = 0;
+    if (lane == 31 && *total) base = atomicAdd(counter, (unsigned long long)*total);
+    return __shfl_sync(0xffffffffu, base, 31);
+}
+
 }  // namespace cpb

@@ -270,6 +270,51 @@ cp_status cp_autotune(cp_prover* p, const cp_refine_opts* opts, int* best, doubl
 /* Selects a level-kernel variant explicitly (0 .. CP_LEVEL_VARIANTS-1). */
 cp_status cp_set_level_variant(cp_prover* p, int family, int precision, int variant);
 
+/* ---------------------------------------------------------------- learned proposal model
+ * The reference has no learned component: these entry points serve the
+ * CP_SPLIT_LEARNED policy and cp_refine_opts.learned_order, which replace the
+ * reference's fixed criterion order (e.g. middle_configuration.cu:196-199) and
+ * its lambda-only split (run_kernel.cuh:110-127) by per-box proposals.  The
+ * model never issues a verdict.  Network per family: 9 box features -> 64 ->
+ * 64 -> 8 logits (4 sub-criterion failure logits, 4 split-axis logits),
+ * tanh-GELU, BF16 tensor-core products with FP32 accumulation.
+ *
+ * cp_model_collect runs cp_refine(opts) (plain policy, no learned options)
+ * and labels every sample_stride-th box of each evaluated chunk, up to
+ * max_records: FULL-mode failure bits and the split axis whose two children
+ * are closest to proved (one-level look-ahead).  The records stay in the
+ * handle (one family at a time). */
+cp_status cp_model_collect(cp_prover* p, const cp_refine_opts* opts, int64_t max_records, int32_t sample_stride,
+                           int64_t* n_records);
+
+/* Copies up to cap records to host memory: feats [cap][16] (BF16 values as
+ * float), crit (failure bits), axis (-1 = no split label), boxes [cap][8]
+ * (lo, hi per axis), depth.  Any pointer may be NULL.  *n = records held. */
+cp_status cp_model_records(cp_prover* p, float* feats, uint8_t* crit, int8_t* axis, double* boxes, uint8_t* depth,
+                           size_t cap, size_t* n);
+
+/* Trains the family's network on the collected records on the GPU: seeded
+ * initialisation and shuffle, batch (a multiple of 64), Adam with learning
+ * rate lr; losses: NULL or epochs floats receiving the mean loss per epoch. */
+cp_status cp_model_train(cp_prover* p, int family, int epochs, int batch, float lr, uint64_t seed, float* losses);
+
+/* FP32 master parameters (cp_model_param_count() floats: W1 [16][64], b1 [64],
+ * W2 [64][64], b2 [64], W3 [64][8], b3 [8]; W rows = inputs). */
+int cp_model_param_count(void);
+cp_status cp_model_get_params(cp_prover* p, int family, float* params);
+cp_status cp_model_set_params(cp_prover* p, int family, const float* params);
+
+/* One forward + backward pass on the GPU over host rows, without an optimiser
+ * step: mean loss and its gradient with respect to the parameters (for
+ * gradient checks).  feats [n][16] FP32 (rounded to BF16 on the device). */
+cp_status cp_model_loss_grad(int family, const float* params, const float* feats, const uint8_t* crit,
+                             const int8_t* axis, size_t n, float* loss, float* grad);
+
+/* Network outputs for host boxes (lo/hi SoA, stride n; depth may be NULL):
+ * logits [n][8], the chosen split axis and criterion order per box. */
+cp_status cp_model_predict(cp_prover* p, int family, const double* lo, const double* hi, const uint8_t* depth,
+                           size_t n, float* logits, uint8_t* axis, uint8_t* order);
+
 /* ---------------------------------------------------------------- no allocation
  * This entry point has no counterpart in the reference.
  *

@@ -69,8 +69,14 @@ def gelu_grad(x):
     return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * GELU_C * (1.0 + 3 * 0.044715 * x * x)
 
 
-def forward(p: np.ndarray, feats: np.ndarray) -> dict:
-    w = unpack(np.asarray(p, np.float32))
+def _ident(x):
+    return np.asarray(x, np.float64)
+
+
+def forward(p: np.ndarray, feats: np.ndarray, exact: bool = False) -> dict:
+    """exact=True skips every BF16 rounding (for finite-difference checks)."""
+    bf16 = _ident if exact else globals()["bf16"]
+    w = unpack(np.asarray(p, np.float64 if exact else np.float32))
     x = bf16(feats)
     h1 = x @ bf16(w["W1"]) + w["b1"]
     g1 = bf16(gelu(h1))
@@ -80,14 +86,15 @@ def forward(p: np.ndarray, feats: np.ndarray) -> dict:
     return dict(x=x, h1=h1, g1=g1, h2=h2, g2=g2, z=z)
 
 
-def loss_grad(family: int, p: np.ndarray, feats: np.ndarray, crit: np.ndarray, axis: np.ndarray):
+def loss_grad(family: int, p: np.ndarray, feats: np.ndarray, crit: np.ndarray, axis: np.ndarray, exact: bool = False):
     """Mean loss over the rows and its gradient with respect to the flat parameters.
 
     crit: uint8 failure bits per row (bit k = sub-criterion k fails);
     axis: int8 best split axis per row, -1 = no label."""
-    K, D = N_CRITERIA[family], DIMS[family]
-    w = unpack(np.asarray(p, np.float32))
-    f = forward(p, feats)
+    K, D = min(N_CRITERIA[family], 4), DIMS[family]
+    bf16 = _ident if exact else globals()["bf16"]
+    w = unpack(np.asarray(p, np.float64 if exact else np.float32))
+    f = forward(p, feats, exact)
     z = f["z"]
     B = z.shape[0]
     y = ((crit[:, None].astype(np.int64) >> np.arange(4)) & 1).astype(np.float64)
