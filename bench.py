@@ -246,36 +246,30 @@ def roofline_of(cp, device, reps_plain) -> dict:
 
 def cpu_baseline(seconds: float) -> dict:
     """The CPU oracle (all host threads) on a bounded sample of the workload:
-    the seed lattices of the six families, sampled uniformly."""
+    boxes drawn uniformly from the seed lattices of the families, in rounds of
+    growing size until about `seconds` of CPU time have been spent."""
     from oracle import oracle as O
 
     threads = os.cpu_count() or 1
     rng = np.random.default_rng(1)
-    total_boxes, t_total = 0, 0.0
-    per_family = 0
-    # calibrate: time a small batch per family, then size the sample to the budget
-    samples = []
-    for f in FAMILIES:
-        dims = DIMS[f]
-        idx = np.sort(rng.choice(SEED_RES ** dims, size=2000, replace=False))
-        samples.append(O.lattice_boxes(f, (0.5, 0.9900000000000001), [SEED_RES] * dims, idx))
-    t0 = time.perf_counter()
-    for f in FAMILIES:
-        O.eval_boxes(f, *samples[f], threads=threads)
-    rate = 6 * 2000 / (time.perf_counter() - t0)
-    per_family = int(max(2000, rate * seconds / 6))
-    for f in FAMILIES:
-        dims = DIMS[f]
-        total = SEED_RES ** dims
-        idx = np.sort(rng.choice(total, size=min(per_family, total), replace=False))
-        lo, hi = O.lattice_boxes(f, (0.5, 0.9900000000000001), [SEED_RES] * dims, idx)
-        t0 = time.perf_counter()
-        O.eval_boxes(f, lo, hi, threads=threads)
-        t_total += time.perf_counter() - t0
-        total_boxes += idx.size
+    total_boxes, t_total, per_family, rounds = 0, 0.0, 4000, 0
+    while t_total < seconds:
+        for f in FAMILIES:
+            dims = DIMS[f]
+            total = SEED_RES ** dims
+            idx = np.sort(rng.choice(total, size=min(per_family, total), replace=False))
+            lo, hi = O.lattice_boxes(f, (0.5, 0.9900000000000001), [SEED_RES] * dims, idx)
+            t0 = time.perf_counter()
+            O.eval_boxes(f, lo, hi, threads=threads)
+            t_total += time.perf_counter() - t0
+            total_boxes += idx.size
+        rounds += 1
+        if t_total < seconds / 3:
+            per_family = min(per_family * 4, 4_000_000)
     return {"value": total_boxes / t_total, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{per_family} boxes per family from the 64^dims seed lattices of all six families, "
-                      f"CPU restatement (oracle/cpu_oracle.cpp), {threads} threads, {t_total:.1f} s"}
+            "sample": f"{total_boxes} boxes drawn from the 64^dims seed lattices of the families "
+                      f"({', '.join(str(f) for f in FAMILIES)}) in {rounds} rounds, CPU restatement "
+                      f"(oracle/cpu_oracle.cpp), {threads} threads, {t_total:.1f} s of evaluation"}
 
 
 def main_reference(args, world, rank):

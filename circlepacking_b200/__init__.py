@@ -183,6 +183,8 @@ def asin_pad(x):
 
 # ---------------------------------------------------------------- prover handle
 SPLIT_UNIFORM, SPLIT_LAMBDA, SPLIT_WIDEST, SPLIT_LEARNED = range(4)
+ENGINE_LEVELS, ENGINE_GRAPH = 0, 1
+GRAPH_BLOCKS, GRAPH_BPT = (64, 128, 256, 512, 1024), (1, 2, 4, 8)
 REFERENCE_SIZES = ((256, 256, 256, 64), (4096, 4096, 4096), (256, 256, 256, 64), (512, 256, 256, 64),
                    (4096, 1024, 1024), (1024, 256, 128, 128))
 
@@ -190,7 +192,8 @@ REFERENCE_SIZES = ((256, 256, 256, 64), (4096, 4096, 4096), (256, 256, 256, 64),
 class RefineOpts(ctypes.Structure):
     _fields_ = [("family", ctypes.c_int32), ("precision", ctypes.c_int32), ("policy", ctypes.c_int32),
                 ("max_depth", ctypes.c_int32), ("seed_sizes", ctypes.c_int32 * 4), ("seed_lambda", ctypes.c_double * 2),
-                ("level_capacity", ctypes.c_int64), ("block", ctypes.c_int32), ("learned_order", ctypes.c_int32)]
+                ("level_capacity", ctypes.c_int64), ("block", ctypes.c_int32), ("learned_order", ctypes.c_int32),
+                ("engine", ctypes.c_int32), ("boxes_per_thread", ctypes.c_int32)]
 
 
 class RefineReport(ctypes.Structure):
@@ -236,14 +239,28 @@ def _declare_handle(L):
     L.cp_autotune.argtypes = [P, ctypes.POINTER(RefineOpts), ctypes.POINTER(ctypes.c_int), P]
     L.cp_refine_boxes_static.argtypes = [I, I, I, I, P, P, P, SZ, ctypes.POINTER(RefineReport), P]
     L.cp_set_level_variant.argtypes = [P, I, I, I]
+    L.cp_autotune_graph.argtypes = [P, ctypes.POINTER(RefineOpts), ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_int), P]
 
 
 def measure_primitives(device: int = 0) -> dict:
     L = lib()
     _declare_handle(L)
-    rates = np.zeros(6, np.float64)
+    rates = np.zeros(7, np.float64)
     _check(L.cp_measure_primitives(device, rates.ctypes.data), "cp_measure_primitives")
-    return dict(zip(("dfma", "dadd_rd", "dmul_rd", "ddiv_rd", "asin", "ffma"), rates.tolist()))
+    return dict(zip(("dfma", "dadd_rd", "dmul_rd", "ddiv_rd", "asin", "ffma", "div_rd_lib"), rates.tolist()))
+
+
+def div_check(a, b):
+    """(library RD, library RU, __ddiv_rd, __ddiv_ru) of a/b on the device, as numpy arrays."""
+    torch = _torch()
+    L = lib()
+    L.cp_div_check.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]
+    a = _dev(a, torch.float64)
+    b = _dev(b, torch.float64)
+    out = torch.empty((a.numel(), 4), dtype=torch.float64, device="cuda")
+    _check(L.cp_div_check(_ptr(a), _ptr(b), a.numel(), _ptr(out), _stream()), "cp_div_check")
+    return out.cpu().numpy().T
 
 
 def _sizes4(sizes):
@@ -285,7 +302,7 @@ class Prover:
 
     @staticmethod
     def opts(family, precision=FP64, policy=SPLIT_UNIFORM, max_depth=2, seed_sizes=None, seed_lambda=None,
-             level_capacity=0, learned_order=False) -> RefineOpts:
+             level_capacity=0, learned_order=False, engine=ENGINE_LEVELS, block=0, boxes_per_thread=0) -> RefineOpts:
         o = RefineOpts()
         o.family, o.precision, o.policy, o.max_depth = family, precision, policy, max_depth
         ss = list(seed_sizes or [64] * DIMS[family]) + [1] * 4
@@ -294,8 +311,10 @@ class Prover:
         sl = seed_lambda or (LAMBDA_MIN, LAMBDA_MAX)
         o.seed_lambda[0], o.seed_lambda[1] = sl
         o.level_capacity = level_capacity
-        o.block = 0
+        o.block = block
         o.learned_order = int(bool(learned_order))
+        o.engine = engine
+        o.boxes_per_thread = boxes_per_thread
         return o
 
     def autotune(self, family, **kw):
@@ -305,6 +324,16 @@ class Prover:
         ms = np.zeros(4, np.float64)
         _check(self._L.cp_autotune(self._h, ctypes.byref(o), ctypes.byref(best), ms.ctypes.data), "cp_autotune")
         return best.value, ms.tolist()
+
+    def autotune_graph(self, family, **kw):
+        """Times every graph-engine kernel shape (block size x boxes per thread) on
+        this refinement and keeps the fastest; returns (block, bpt, ms[5][4])."""
+        o = self.opts(family, **kw)
+        blk, bpt = ctypes.c_int(), ctypes.c_int()
+        ms = np.zeros(20, np.float64)
+        _check(self._L.cp_autotune_graph(self._h, ctypes.byref(o), ctypes.byref(blk), ctypes.byref(bpt),
+                                         ms.ctypes.data), "cp_autotune_graph")
+        return blk.value, bpt.value, ms.reshape(5, 4).tolist()
 
     def set_level_variant(self, family, precision, variant):
         _check(self._L.cp_set_level_variant(self._h, family, precision, variant), "cp_set_level_variant")

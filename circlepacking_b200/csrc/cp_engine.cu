@@ -12,6 +12,7 @@
 
 #include "cp_common.h"
 #include "cp_engine.h"
+#include "cp_graph_kernels.cuh"
 #include "cp_level.cuh"
 
 using namespace cpb;
@@ -87,6 +88,59 @@ __global__ void k_single_table(double lo, double h, int n, double* t, double* v)
         t[i] = x;
         v[i] = single_placement(x);
     }
+}
+
+// The device-side scheduler of the graph-driven loop (one thread): commits the
+// previous chunk (input consumed, children appended), then picks the next
+// chunk exactly as the host loop does -- the deepest non-empty level, as many
+// boxes as the next level has room for -- or ends the loop.
+constexpr unsigned long long kGraphLaunchLimit = 1ull << 22;
+__global__ void k_sched(DevSched* s, unsigned long long* cnt, cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    DevJob& j = s->job;
+    if (j.count) {
+        s->n[j.in_level] -= j.count;
+        if (j.out_level >= 0) s->n[j.out_level] = cnt[C_OUT];
+        j.count = 0;
+        if (cnt[C_ERR] & E_OVERFLOW) {
+            s->status = 1;
+            cudaGraphSetConditional(h, 0);
+            return;
+        }
+    }
+    int l = -1;
+    for (int k = s->nlevels - 1; k >= 0; --k)
+        if (s->n[k]) {
+            l = k;
+            break;
+        }
+    if (l < 0) {
+        cudaGraphSetConditional(h, 0);
+        return;
+    }
+    if (s->launches >= kGraphLaunchLimit) {  // bound on the loop (cannot be reached by a valid schedule)
+        s->status = 2;
+        cudaGraphSetConditional(h, 0);
+        return;
+    }
+    const int out = (l + 1 < s->nlevels && l < s->max_depth) ? l + 1 : -1;
+    unsigned long long c = s->n[l];
+    if (out >= 0) {
+        const unsigned long long room = (s->cap - s->n[out]) / (unsigned long long)s->fanout;
+        if (room < c) c = room;
+        if (c == 0) {
+            s->status = 1;
+            cudaGraphSetConditional(h, 0);
+            return;
+        }
+    }
+    j.in_level = l;
+    j.out_level = out;
+    j.begin = s->n[l] - c;
+    j.count = c;
+    cnt[C_OUT] = out >= 0 ? s->n[out] : 0;
+    s->claim = 0;
+    s->launches += 1;
 }
 
 // ------------------------------------------------------------------ reference step
@@ -203,6 +257,15 @@ struct cp_prover {
     int levels_dims = 0;
     size_t level_cap = 0;
     void* model = nullptr;  // learned model state (cp_model.cu)
+    // device-driven loop (CUDA graph with a conditional WHILE node)
+    BoxList* d_levels = nullptr;
+    DevSched* d_sched = nullptr;
+    DevSched* h_sched = nullptr;  // pinned mirror
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    unsigned long long graph_key[11] = {0};
+    int graph_variant[6][2] = {{1, 1}, {1, 1}, {1, 1}, {1, 1}, {1, 1}, {1, 1}};  // block-size variant
+    int graph_bpt[6][2] = {{2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}};      // boxes per thread
     int variant[6][2] = {{1, 1}, {0, 0}, {1, 1}, {1, 1}, {0, 0}, {1, 1}};  // level-kernel variant per family/precision
 };
 
@@ -465,11 +528,146 @@ cp_status refine_levels(cp_prover* p, const cp_refine_opts& o, cp_refine_report*
     return CP_OK;
 }
 
+void free_graph(cp_prover* p) {
+    if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    p->graph_exec = nullptr;
+    p->graph = nullptr;
+    std::memset(p->graph_key, 0, sizeof(p->graph_key));
+}
+
+int graph_variant_of_block(int block) {
+    for (int v = 0; v < kGraphVariants; ++v)
+        if (kGraphBlock[v] == block) return v;
+    return -1;
+}
+
+// Builds the graph of the device-driven loop: a WHILE node whose body is
+// scheduler -> (model hints) -> persistent level kernel.
+cp_status build_graph(cp_prover* p, const cp_refine_opts& o, int variant, int bpt, bool learned_axis,
+                      bool learned_order) {
+    free_graph(p);
+    const int fam = o.family;
+    const int prec = o.precision ? 1 : 0;
+    CP_TRY(cuda_ok(cudaGraphCreate(&p->graph, 0)));
+    cudaGraphConditionalHandle h;
+    CP_TRY(cuda_ok(cudaGraphConditionalHandleCreate(&h, p->graph, 1, cudaGraphCondAssignDefault)));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CP_TRY(cuda_ok(cudaGraphAddNode(&node, p->graph, nullptr, 0, &cp)));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CP_TRY(cuda_ok(cudaStreamBeginCaptureToGraph(p->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)));
+    cp_status st = CP_OK;
+    do {
+        k_sched<<<1, 32, 0, p->stream>>>(p->d_sched, p->cnt, h);
+        if ((st = cp_check_launch()) != CP_OK) break;
+        uint8_t *axis = nullptr, *order = nullptr;
+        if (learned_axis || learned_order) {
+            st = cp_model_graph_hints(p, fam, p->d_sched, p->d_levels, p->level_cap, learned_axis ? &axis : nullptr,
+                                      learned_order ? &order : nullptr);
+            if (st != CP_OK) break;
+        }
+        PersistArgs pa;
+        pa.levels = p->d_levels;
+        pa.sched = p->d_sched;
+        pa.cnt = p->cnt;
+        pa.per_depth = p->per_depth;
+        pa.tab = table_of(p);
+        pa.policy = o.policy == CP_SPLIT_LEARNED ? SPLIT_GIVEN : o.policy;
+        pa.max_depth = o.max_depth;
+        pa.bpt = bpt;
+        pa.axis_hint = axis;
+        pa.order_hint = order;
+        void* kern = prec ? cp_graph_kernel_fp32(fam, variant) : cp_graph_kernel_fp64(fam, variant);
+        const int block = kGraphBlock[variant];
+        int per_sm = 0, sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+        void* args[] = {&pa};
+        st = cuda_ok(cudaLaunchKernel(kern, dim3((unsigned)(sms * per_sm)), dim3((unsigned)block), args, 0, p->stream));
+    } while (0);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(p->stream, &captured);
+    if (st != CP_OK) return st;
+    CP_TRY(cuda_ok(ec));
+    return cuda_ok(cudaGraphInstantiate(&p->graph_exec, p->graph, 0));
+}
+
+// The level-stack loop of refine_levels, run on the device by one CUDA graph
+// launch: no host round trip between chunks.
+cp_status refine_graph(cp_prover* p, const cp_refine_opts& o, cp_refine_report* r, double t_wall0) {
+    const int fam = o.family;
+    const int D = family_dims(fam);
+    const int prec = o.precision ? 1 : 0;
+    const int nlevels = (int)p->levels.size();
+    if (nlevels > kMaxLevels) return cp_fail(CP_ERR_INVALID, "graph engine: max_depth must be < %d", kMaxLevels);
+    int variant = o.block > 0 ? graph_variant_of_block(o.block) : p->graph_variant[fam][prec];
+    if (variant < 0) return cp_fail(CP_ERR_INVALID, "graph engine: block must be 64, 128, 256, 512 or 1024");
+    const int bpt = o.boxes_per_thread > 0 ? o.boxes_per_thread : p->graph_bpt[fam][prec];
+    if (bpt > 8) return cp_fail(CP_ERR_INVALID, "graph engine: boxes_per_thread must be 1..8");
+    const bool learned_axis = o.policy == CP_SPLIT_LEARNED, learned_order = o.learned_order != 0;
+    if (!p->d_levels) {
+        CP_TRY(cuda_ok(cudaMalloc(&p->d_levels, sizeof(BoxList) * kMaxLevels)));
+        CP_TRY(cuda_ok(cudaMalloc(&p->d_sched, sizeof(DevSched))));
+        CP_TRY(cuda_ok(cudaMallocHost(&p->h_sched, sizeof(DevSched))));
+    }
+    BoxList hl[kMaxLevels];
+    for (int l = 0; l < nlevels; ++l) hl[l] = p->levels[l].b;
+    DevSched& hs = *p->h_sched;
+    std::memset(&hs, 0, sizeof(hs));
+    for (int l = 0; l < nlevels; ++l) hs.n[l] = p->levels[l].n;
+    hs.cap = p->level_cap;
+    hs.nlevels = nlevels;
+    hs.max_depth = o.max_depth;
+    hs.fanout = fanout(o.policy == CP_SPLIT_LEARNED ? SPLIT_GIVEN : o.policy, D);
+    CP_TRY(cuda_ok(cudaMemcpyAsync(p->d_levels, hl, sizeof(BoxList) * nlevels, cudaMemcpyHostToDevice, p->stream)));
+    CP_TRY(cuda_ok(cudaMemcpyAsync(p->d_sched, &hs, sizeof(DevSched), cudaMemcpyHostToDevice, p->stream)));
+    if (learned_axis || learned_order) CP_TRY(cp_model_reserve_hints(p, p->level_cap));
+    const unsigned long long key[11] = {(unsigned long long)fam + 1, (unsigned long long)prec, (unsigned long long)variant,
+                                        (unsigned long long)bpt, (unsigned long long)o.policy,
+                                        (unsigned long long)o.max_depth,
+                                        (unsigned long long)(learned_axis | (learned_order << 1)),
+                                        (unsigned long long)(uintptr_t)p->levels[0].b.lo, (unsigned long long)p->level_cap,
+                                        (unsigned long long)nlevels,
+                                        (unsigned long long)(uintptr_t)cp_model_hint_buffer(p)};
+    if (!p->graph_exec || std::memcmp(key, p->graph_key, sizeof(key)) != 0) {
+        CP_TRY(build_graph(p, o, variant, bpt, learned_axis, learned_order));
+        std::memcpy(p->graph_key, key, sizeof(key));
+    }
+    CP_TRY(cuda_ok(cudaEventRecord(p->ev0, p->stream)));
+    CP_TRY(cuda_ok(cudaGraphLaunch(p->graph_exec, p->stream)));
+    CP_TRY(cuda_ok(cudaEventRecord(p->ev1, p->stream)));
+    CP_TRY(cuda_ok(cudaMemcpyAsync(p->h_sched, p->d_sched, sizeof(DevSched), cudaMemcpyDeviceToHost, p->stream)));
+    CP_TRY(read_counters(p));
+    float t = 0;
+    cudaEventElapsedTime(&t, p->ev0, p->ev1);
+    for (int l = 0; l < nlevels; ++l) p->levels[l].n = (size_t)p->h_sched->n[l];
+    if (p->h_sched->status == 1) return cp_fail(CP_ERR_CAPACITY, "graph engine: worklist level capacity exceeded");
+    if (p->h_sched->status != 0) return cp_fail(CP_ERR_DEVICE, "graph engine: scheduler stopped (status %d)",
+                                                p->h_sched->status);
+    cp_engine_fill_report(p->h_cnt, r);
+    r->launches = (int32_t)p->h_sched->launches;
+    r->device_ms = t;
+    r->wall_ms = now_ms() - t_wall0;
+    return CP_OK;
+}
+
+cp_status run_refinement(cp_prover* p, const cp_refine_opts& o, cp_refine_report* r, double t0) {
+    if (o.engine == CP_ENGINE_GRAPH && !cp_model_collecting(p)) return refine_graph(p, o, r, t0);
+    return refine_levels(p, o, r, t0);
+}
+
 cp_status check_opts(const cp_refine_opts* o) {
     if (!o || o->family < 0 || o->family > 5) return CP_ERR_INVALID;
     if (o->precision != CP_FP64 && o->precision != CP_FP32_PREFILTER) return CP_ERR_INVALID;
     if (o->policy < CP_SPLIT_UNIFORM || o->policy > CP_SPLIT_LEARNED) return CP_ERR_INVALID;
     if (o->max_depth < 0 || o->max_depth > 250) return CP_ERR_INVALID;
+    if (o->engine != CP_ENGINE_LEVELS && o->engine != CP_ENGINE_GRAPH) return CP_ERR_INVALID;
+    if (o->boxes_per_thread < 0 || o->boxes_per_thread > 8) return CP_ERR_INVALID;
     return CP_OK;
 }
 
@@ -519,6 +717,10 @@ void cp_destroy(cp_prover* p) {
     cudaSetDevice(p->device);
     if (p->stream) cudaStreamSynchronize(p->stream);
     cp_model_free(p);
+    free_graph(p);
+    cudaFree(p->d_levels);
+    cudaFree(p->d_sched);
+    cudaFreeHost(p->h_sched);
     free_levels(p);
     cudaFree(p->cnt);
     cudaFreeHost(p->h_cnt);
@@ -562,7 +764,7 @@ cp_status cp_refine(cp_prover* p, const cp_refine_opts* o, cp_refine_report* r) 
     CP_TRY(cp_check_launch());
     p->levels[0].n = total;
     CP_TRY(reset_counters(p));
-    return refine_levels(p, *o, r, t0);
+    return run_refinement(p, *o, r, t0);
 }
 
 cp_status cp_set_level_variant(cp_prover* p, int family, int precision, int variant) {
@@ -594,6 +796,36 @@ cp_status cp_autotune(cp_prover* p, const cp_refine_opts* o, int* best, double* 
     return CP_OK;
 }
 
+cp_status cp_autotune_graph(cp_prover* p, const cp_refine_opts* o, int* block, int* boxes_per_thread, double* ms) {
+    if (!p || !block || !boxes_per_thread) return CP_ERR_INVALID;
+    CP_TRY(check_opts(o));
+    static const int kBpt[4] = {1, 2, 4, 8};
+    cp_refine_opts t = *o;
+    t.engine = CP_ENGINE_GRAPH;
+    double best_ms = 1e300;
+    int best_v = 1, best_b = 2;
+    for (int v = 0; v < kGraphVariants; ++v)
+        for (int b = 0; b < 4; ++b) {
+            t.block = kGraphBlock[v];
+            t.boxes_per_thread = kBpt[b];
+            cp_refine_report r;
+            CP_TRY(cp_refine(p, &t, &r));  // warm-up (also builds the graph)
+            CP_TRY(cp_refine(p, &t, &r));
+            if (ms) ms[v * 4 + b] = r.device_ms;
+            if (r.device_ms < best_ms) {
+                best_ms = r.device_ms;
+                best_v = v;
+                best_b = kBpt[b];
+            }
+        }
+    const int pr = o->precision ? 1 : 0;
+    p->graph_variant[o->family][pr] = best_v;
+    p->graph_bpt[o->family][pr] = best_b;
+    *block = kGraphBlock[best_v];
+    *boxes_per_thread = best_b;
+    return CP_OK;
+}
+
 cp_status cp_refine_boxes(cp_prover* p, const cp_refine_opts* o, const double* lo, const double* hi,
                           const uint8_t* depth, size_t n, cp_refine_report* r) {
     if (!p || !r || (n && (!lo || !hi))) return CP_ERR_INVALID;
@@ -614,7 +846,7 @@ cp_status cp_refine_boxes(cp_prover* p, const cp_refine_opts* o, const double* l
     CP_TRY(reset_counters(p));
     // explicit seeds may carry depths above zero: they stay in level 0's buffer
     // and their children go to level 1; max_depth compares with the box depth
-    return refine_levels(p, *o, r, t0);
+    return run_refinement(p, *o, r, t0);
 }
 
 cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* o, const double* lo, const double* hi,
@@ -642,7 +874,7 @@ cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* o, const doub
     }
     p->levels[0].n = n;
     CP_TRY(reset_counters(p));
-    return refine_levels(p, *o, r, t0);
+    return run_refinement(p, *o, r, t0);
 }
 
 cp_status cp_reference_step(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,

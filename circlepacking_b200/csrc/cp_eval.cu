@@ -68,6 +68,18 @@ __global__ void __launch_bounds__(kEvalBlock) k_eval_prefilter(const double* __r
     }
 }
 
+// The library's directed division against the CUDA intrinsics it replaces.
+__global__ void k_div_check(const double* __restrict__ a, const double* __restrict__ b, size_t n,
+                            double* __restrict__ out) {
+    const size_t step = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step) {
+        out[4 * i + 0] = div_rd(a[i], b[i]);
+        out[4 * i + 1] = div_ru(a[i], b[i]);
+        out[4 * i + 2] = __ddiv_rd(a[i], b[i]);
+        out[4 * i + 3] = __ddiv_ru(a[i], b[i]);
+    }
+}
+
 __global__ void k_single_placement(const double* __restrict__ lam, size_t n, double* __restrict__ out) {
     const size_t step = (size_t)gridDim.x * blockDim.x;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step) out[i] = single_placement(lam[i]);
@@ -299,6 +311,13 @@ cp_status cp_asin_pad(const double* x, size_t n, double* rd, double* ru, void* s
     if (n == 0) return CP_OK;
     if (!x || !rd || !ru) return CP_ERR_INVALID;
     k_asin_pad<<<grid_for(k_asin_pad, n, 128), 128, 0, (cudaStream_t)stream>>>(x, n, rd, ru);
+    return cp_check_launch();
+}
+
+cp_status cp_div_check(const double* a, const double* b, size_t n, double* out, void* stream) {
+    if (n == 0) return CP_OK;
+    if (!a || !b || !out) return CP_ERR_INVALID;
+    k_div_check<<<grid_for(k_div_check, n, 128), 128, 0, (cudaStream_t)stream>>>(a, b, n, out);
     return cp_check_launch();
 }
 

@@ -85,6 +85,61 @@ __device__ __forceinline__ double asin_ru(double x) {
     return y;
 }
 
+// ------------------------------------------------------------------ directed division
+// a / b rounded toward -inf (DOWN) or +inf, bit-identical to __ddiv_rd /
+// __ddiv_ru.  Method (Markstein's FMA division, certified by exact remainders):
+//   y  ~ 1/b       hardware reciprocal approximation + two Newton steps
+//   q  = RN-ish(a/b)  q0 = a*y, refined once with the remainder a - q0*b
+//   the sign of t - c for the true quotient t = a/b and a candidate c is the
+//   sign of (a - c*b) / b; a - c*b is computed by one FMA and, for operands
+//   with |a|, |b| in [2^-500, 2^500], its rounded value has the exact sign
+//   (the exact difference is a multiple of 2^-606 or zero, far above the
+//   underflow threshold).  With q and its neighbour n in the direction of t,
+//   t in [q, n] (or [n, q]) is certified, which fixes both directed results.
+// Operands outside that range, and the (not expected) case where the
+// candidate is more than one unit in the last place away, use the intrinsic.
+__device__ __forceinline__ bool div_in_range(double a, double b) {
+    const unsigned ea = ((unsigned)__double2hiint(a) >> 20) & 0x7ffu;
+    const unsigned eb = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
+    return (ea - 523u) <= 1000u && (eb - 523u) <= 1000u;
+}
+// neighbours of a finite, normal, nonzero q (never crossing zero or infinity)
+__device__ __forceinline__ double next_up(double q) {
+    const long long b = __double_as_longlong(q);
+    return __longlong_as_double(q > 0.0 ? b + 1 : b - 1);
+}
+__device__ __forceinline__ double next_down(double q) {
+    const long long b = __double_as_longlong(q);
+    return __longlong_as_double(q > 0.0 ? b - 1 : b + 1);
+}
+template <bool UP>
+__device__ __forceinline__ double div_dir(double a, double b) {
+    if (!div_in_range(a, b)) return UP ? __ddiv_ru(a, b) : __ddiv_rd(a, b);
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    double e = __fma_rn(-b, y, 1.0);
+    y = __fma_rn(y, e, y);
+    e = __fma_rn(-b, y, 1.0);
+    if (!(fabs(e) < 1e-6)) return UP ? __ddiv_ru(a, b) : __ddiv_rd(a, b);  // reciprocal not close: no certificate
+    y = __fma_rn(y, e, y);
+    double q = __dmul_rn(a, y);
+    q = __fma_rn(__fma_rn(-q, b, a), y, q);
+    const double r = __fma_rn(-q, b, a);
+    if (r == 0.0) return q;  // exact quotient
+    const bool bneg = b < 0.0;
+    const bool above = (r > 0.0) != bneg;  // t > q
+    const double n = above ? next_up(q) : next_down(q);
+    const double rn = __fma_rn(-n, b, a);
+    if (rn == 0.0) return n;  // t == n exactly
+    const bool n_beyond = above ? ((rn < 0.0) != bneg) : ((rn > 0.0) != bneg);  // t strictly between q and n
+    if (!n_beyond) return UP ? __ddiv_ru(a, b) : __ddiv_rd(a, b);
+    // t in (q, n) when above, else in (n, q)
+    if (UP) return above ? n : q;
+    return above ? q : n;
+}
+__device__ __forceinline__ double div_rd(double a, double b) { return div_dir<false>(a, b); }
+__device__ __forceinline__ double div_ru(double a, double b) { return div_dir<true>(a, b); }
+
 // ------------------------------------------------------------------ interval ops
 __device__ __forceinline__ Iv pt(double x) { return {x, x}; }
 __device__ __forceinline__ Iv iadd(Iv a, Iv b) { return {__dadd_rd(a.lo, b.lo), __dadd_ru(a.hi, b.hi)}; }
@@ -107,13 +162,13 @@ __device__ __forceinline__ Iv isq(Iv x) {
 }
 // interval.cuh:277-310, one bound at a time
 __device__ __forceinline__ double idiv_lo(Iv a, Iv o) {
-    if (o.lo > 0) return a.lo >= 0 ? __ddiv_rd(a.lo, o.hi) : __ddiv_rd(a.lo, o.lo);
-    if (o.hi < 0) return (a.lo >= 0 || !(a.hi <= 0)) ? __ddiv_rd(a.hi, o.hi) : __ddiv_rd(a.hi, o.lo);
+    if (o.lo > 0) return a.lo >= 0 ? div_rd(a.lo, o.hi) : div_rd(a.lo, o.lo);
+    if (o.hi < 0) return (a.lo >= 0 || !(a.hi <= 0)) ? div_rd(a.hi, o.hi) : div_rd(a.hi, o.lo);
     return -__longlong_as_double(0x7ff0000000000000ll);
 }
 __device__ __forceinline__ double idiv_hi(Iv a, Iv o) {
-    if (o.lo > 0) return (a.lo >= 0 || !(a.hi <= 0)) ? __ddiv_ru(a.hi, o.lo) : __ddiv_ru(a.hi, o.hi);
-    if (o.hi < 0) return a.lo >= 0 ? __ddiv_ru(a.lo, o.lo) : __ddiv_ru(a.lo, o.hi);
+    if (o.lo > 0) return (a.lo >= 0 || !(a.hi <= 0)) ? div_ru(a.hi, o.lo) : div_ru(a.hi, o.hi);
+    if (o.hi < 0) return a.lo >= 0 ? div_ru(a.lo, o.lo) : div_ru(a.lo, o.hi);
     return __longlong_as_double(0x7ff0000000000000ll);
 }
 __device__ __forceinline__ Iv idiv(Iv a, Iv o) { return {idiv_lo(a, o), idiv_hi(a, o)}; }
@@ -299,23 +354,23 @@ __device__ __forceinline__ Iv ca_inner_outer(Iv la, Iv ra, Iv rb, bool& t) {
     return {ca_mixed_lo<false>(la, ra, rb, t), ca_mixed_hi<false>(la, ra, rb, t)};
 }
 // collision_angles.cu:233-246, one bound at a time
-__device__ __forceinline__ double semi_outer_lo(Iv r) { return asin_rd(__ddiv_rd(r.lo, __dadd_ru(1.0, -r.lo))); }
-__device__ __forceinline__ double semi_outer_hi(Iv r) { return asin_ru(__ddiv_ru(r.hi, __dadd_rd(1.0, -r.hi))); }
-__device__ __forceinline__ double semi_inner_lo(Iv la, Iv r) { return asin_rd(__ddiv_rd(r.lo, __dadd_ru(la.hi, r.lo))); }
-__device__ __forceinline__ double semi_inner_hi(Iv la, Iv r) { return asin_ru(__ddiv_ru(r.hi, __dadd_rd(la.lo, r.hi))); }
+__device__ __forceinline__ double semi_outer_lo(Iv r) { return asin_rd(div_rd(r.lo, __dadd_ru(1.0, -r.lo))); }
+__device__ __forceinline__ double semi_outer_hi(Iv r) { return asin_ru(div_ru(r.hi, __dadd_rd(1.0, -r.hi))); }
+__device__ __forceinline__ double semi_inner_lo(Iv la, Iv r) { return asin_rd(div_rd(r.lo, __dadd_ru(la.hi, r.lo))); }
+__device__ __forceinline__ double semi_inner_hi(Iv la, Iv r) { return asin_ru(div_ru(r.hi, __dadd_rd(la.lo, r.hi))); }
 
 // lower_bound_radius_single_placement.cu:26-61: bisection for the smallest
 // radius r with r^2/asin(r/(1-r)) >= (critical_ratio/pi) (1 - lambda^2).
 __device__ inline double single_placement(double lb_lambda) {
-    const double f = __ddiv_ru(kCriticalRatio, kLbPi);
+    const double f = div_ru(kCriticalRatio, kLbPi);
     const double rhs = __dmul_ru(f, __dadd_ru(1.0, -__dmul_rd(lb_lambda, lb_lambda)));
     double ub = 0.25, lb = 5.0e-324;
     for (int it = 0; it < 2100; ++it) {
         double mid = __dmul_rn(0.5, __dadd_rn(lb, ub));
         if (mid <= lb || mid >= ub) return ub;
         double r_sq = __dmul_rd(mid, mid);
-        double q = __ddiv_ru(mid, __dadd_rd(1.0, -mid));
-        double lhs = __ddiv_rd(r_sq, asin_ru(q));
+        double q = div_ru(mid, __dadd_rd(1.0, -mid));
+        double lhs = div_rd(r_sq, asin_ru(q));
         if (lhs >= rhs)
             ub = mid;
         else

@@ -6,6 +6,7 @@
 #pragma once
 #include <cstdint>
 
+#include "cp_prover.h"
 #include "cp_fp32.cuh"
 #include "cp_worklist.cuh"
 
@@ -51,12 +52,7 @@ struct LevelSmem {
     unsigned long long hist[8];
     unsigned long long depth[kDepthBins];
     unsigned long long handles;
-    // per-warp staging of the parents of one iteration's children
-    struct Parent {
-        double lo[4], hi[4];
-    } par[WARPS][32];
-    uint16_t excl[WARPS][32];
-    uint8_t axis[WARPS][32], dep[WARPS][32];
+    // per warp: the lane owning each slot of one iteration's children
     uint8_t own[WARPS][32 * 16];
 };
 
@@ -129,36 +125,33 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
         if (wbase + total > a.out.cap) {
             if (lane == 0) atomicOr(&a.cnt[C_ERR], E_OVERFLOW);
         } else {
-            if (nchild) {
-#pragma unroll
-                for (int d = 0; d < D; ++d) {
-                    sm.par[w][lane].lo[d] = lo[d];
-                    sm.par[w][lane].hi[d] = hi[d];
-                }
-                sm.excl[w][lane] = (uint16_t)excl;
-                sm.axis[w][lane] = (uint8_t)axis;
-                sm.dep[w][lane] = (uint8_t)depth;
-                for (unsigned c = 0; c < nchild; ++c) sm.own[w][excl + c] = (uint8_t)lane;
-            }
+            // slot -> owning lane; the parent box itself comes from the owner by shuffles
+            for (unsigned c = 0; c < nchild; ++c) sm.own[w][excl + c] = (uint8_t)lane;
             __syncwarp();
-            for (unsigned k = lane; k < total; k += 32) {
-                const int own = sm.own[w][k];
-                const int c = (int)k - (int)sm.excl[w][own];
+            for (unsigned base = 0; base < total; base += 32) {
+                const unsigned k = base + lane;
+                const bool valid = k < total;
+                const int own = valid ? sm.own[w][k] : 0;
                 double plo[4], phi[4], clo[4], chi[4];
 #pragma unroll
                 for (int d = 0; d < D; ++d) {
-                    plo[d] = sm.par[w][own].lo[d];
-                    phi[d] = sm.par[w][own].hi[d];
+                    plo[d] = __shfl_sync(0xffffffffu, lo[d], own);
+                    phi[d] = __shfl_sync(0xffffffffu, hi[d], own);
                 }
-                make_child<D>(plo, phi, a.policy, sm.axis[w][own], c, clo, chi);
-                const bool alive = clip_child<FAM>(clo, chi, a.tab);
-                const size_t o = (size_t)(wbase + k);
+                const int c = (int)k - (int)__shfl_sync(0xffffffffu, excl, own);
+                const int pax = __shfl_sync(0xffffffffu, axis, own);
+                const int pdep = __shfl_sync(0xffffffffu, depth, own);
+                if (valid) {
+                    make_child<D>(plo, phi, a.policy, pax, c, clo, chi);
+                    const bool alive = clip_child<FAM>(clo, chi, a.tab);
+                    const size_t o = (size_t)(wbase + k);
 #pragma unroll
-                for (int d = 0; d < D; ++d) {
-                    a.out.lo[d * a.out.cap + o] = clo[d];
-                    a.out.hi[d * a.out.cap + o] = chi[d];
+                    for (int d = 0; d < D; ++d) {
+                        a.out.lo[d * a.out.cap + o] = clo[d];
+                        a.out.hi[d * a.out.cap + o] = chi[d];
+                    }
+                    a.out.depth[o] = alive ? (uint8_t)(pdep + 1) : (uint8_t)0xFF;
                 }
-                a.out.depth[o] = alive ? (uint8_t)(sm.dep[w][own] + 1) : (uint8_t)0xFF;
             }
             __syncwarp();
         }
@@ -177,5 +170,29 @@ __device__ __forceinline__ void level_flush(const LevelArgs& a, LevelSmem<WARPS>
     for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x)
         if (sm.depth[t]) atomicAdd(&a.per_depth[t], sm.depth[t]);
 }
+
+}  // namespace cpb
+
+namespace cpb {
+
+// ------------------------------------------------------------------ device-driven loop
+// The level-stack schedule of the refinement, kept in device memory so that a
+// CUDA graph can run the whole loop without returning to the host.
+constexpr int kMaxLevels = 64;
+
+struct DevJob {
+    int in_level, out_level;  // out_level < 0: the input level is the last one (no children)
+    unsigned long long begin, count;
+};
+
+struct DevSched {
+    unsigned long long n[kMaxLevels];  // boxes held per level
+    DevJob job;                        // the chunk being evaluated
+    unsigned long long claim;          // next box of the job handed to a warp
+    unsigned long long launches;       // chunks scheduled
+    unsigned long long cap;            // boxes per level buffer
+    int nlevels, max_depth, fanout;
+    int status;                        // 0 ok, 1 worklist capacity exceeded
+};
 
 }  // namespace cpb

@@ -30,7 +30,7 @@
 
 #include "cp_common.h"
 #include "cp_engine.h"
-#include "cp_worklist.cuh"
+#include "cp_level.cuh"
 
 using namespace cpb;
 
@@ -497,6 +497,8 @@ __global__ void k_adam(float* __restrict__ master, float* __restrict__ m, float*
 struct InferArgs {
     BoxList in;
     size_t begin, count;
+    const DevSched* sched;   // graph mode: take in/begin/count from the scheduler's job
+    const BoxList* levels;
     const bf16* views;
     const float* master;
     uint8_t* axis;     // per box, indexed from `begin` (may be null)
@@ -516,6 +518,13 @@ template <int FAM>
 __global__ void __launch_bounds__(128) k_infer(InferArgs a) {
     constexpr int D = family_dims(FAM);
     __shared__ InferSmem s;
+    if (a.sched) {
+        const DevJob job = a.sched->job;
+        if (job.count == 0) return;
+        a.in = a.levels[job.in_level];
+        a.begin = job.begin;
+        a.count = job.count;
+    }
     load_fwd(s.f, a.views, a.master);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -806,6 +815,20 @@ cp_status launch_infer_t(const InferArgs& a, cudaStream_t st) {
     k_infer<FAM><<<grid, 128, 0, st>>>(a);
     return cp_check_launch();
 }
+template <int FAM>
+void k_inferv_t(const InferArgs& a, cudaStream_t st) {
+    k_infer<FAM><<<148 * 4, 128, 0, st>>>(a);
+}
+void k_inferv(int fam, const InferArgs& a, cudaStream_t st) {
+    switch (fam) {
+    case 0: k_inferv_t<0>(a, st); break;
+    case 1: k_inferv_t<1>(a, st); break;
+    case 2: k_inferv_t<2>(a, st); break;
+    case 3: k_inferv_t<3>(a, st); break;
+    case 4: k_inferv_t<4>(a, st); break;
+    default: k_inferv_t<5>(a, st); break;
+    }
+}
 cp_status launch_infer(int fam, const InferArgs& a, cudaStream_t st) {
     switch (fam) {
     case 0: return launch_infer_t<0>(a, st);
@@ -856,12 +879,62 @@ cp_status cp_model_hints(cp_prover* p, int fam, const BoxList& in, size_t begin,
     a.count = count;
     a.views = m->fam[fam].views;
     a.master = m->fam[fam].master;
+    a.sched = nullptr;
+    a.levels = nullptr;
     a.axis = axis ? m->hint_axis : nullptr;
     a.order = order ? m->hint_order : nullptr;
     a.logits = nullptr;
     M_TRY(launch_infer(fam, a, cp_prover_stream(p)));
     if (axis) *axis = m->hint_axis;
     if (order) *order = m->hint_order;
+    return CP_OK;
+}
+
+cp_status cp_model_graph_hints(cp_prover* p, int fam, const DevSched* sched, const BoxList* levels, size_t cap,
+                               uint8_t** axis, uint8_t** order) {
+    ModelState* m = state(p, false);
+    if (!m || !m->fam[fam].ready)
+        return cp_fail(CP_ERR_INVALID, "no proposal model for family %d: train one (cp_model_train) or load "
+                                       "parameters (cp_model_set_params)", fam);
+    if (m->hint_cap < cap) {
+        // allocation is not allowed during stream capture: callers size the
+        // buffers before capturing (cp_model_reserve_hints)
+        return cp_fail(CP_ERR_INVALID, "hint buffers not reserved for %zu boxes", cap);
+    }
+    InferArgs a;
+    a.in = BoxList{nullptr, nullptr, nullptr, 0};
+    a.begin = 0;
+    a.count = 0;
+    a.sched = sched;
+    a.levels = levels;
+    a.views = m->fam[fam].views;
+    a.master = m->fam[fam].master;
+    a.axis = axis ? m->hint_axis : nullptr;
+    a.order = order ? m->hint_order : nullptr;
+    a.logits = nullptr;
+    // grid independent of the (device-side) count: one resident wave
+    k_inferv(fam, a, cp_prover_stream(p));
+    M_TRY(cp_check_launch());
+    if (axis) *axis = m->hint_axis;
+    if (order) *order = m->hint_order;
+    return CP_OK;
+}
+
+const void* cp_model_hint_buffer(cp_prover* p) {
+    ModelState* m = state(p, false);
+    return m ? (const void*)m->hint_axis : nullptr;
+}
+
+cp_status cp_model_reserve_hints(cp_prover* p, size_t cap) {
+    ModelState* m = state(p, false);
+    if (!m) return CP_OK;
+    if (m->hint_cap >= cap) return CP_OK;
+    cudaFree(m->hint_axis);
+    m->hint_axis = nullptr;
+    m->hint_cap = 0;
+    M_TRY(ok_or(cudaMalloc(&m->hint_axis, 2 * cap)));
+    m->hint_order = m->hint_axis + cap;
+    m->hint_cap = cap;
     return CP_OK;
 }
 
@@ -1116,6 +1189,8 @@ cp_status cp_model_predict(cp_prover* p, int family, const double* lo, const dou
             a.in = BoxList{dlo, dhi, dd, n};
             a.begin = 0;
             a.count = n;
+            a.sched = nullptr;
+            a.levels = nullptr;
             a.views = m->fam[family].views;
             a.master = m->fam[family].master;
             a.axis = dax;

@@ -178,8 +178,19 @@ typedef struct cp_refine_opts {
     double seed_lambda[2];  /* outer lambda interval of the lattice seed */
     int64_t level_capacity; /* boxes per level buffer; 0 = 1<<25 */
     int32_t block;          /* threads per block of the level kernel; 0 = 128 */
-    int32_t learned_order;  /* 1 = learned criterion order (needs cp_load_model) */
+    int32_t learned_order;  /* 1 = learned criterion order (needs a trained or loaded model) */
+    int32_t engine;         /* cp_engine: host-driven level loop or one CUDA graph launch */
+    int32_t boxes_per_thread; /* graph engine: boxes a warp lane takes per claim (1..8); 0 = tuned */
 } cp_refine_opts;
+
+/* Refinement engines.  CP_ENGINE_LEVELS: the host picks each chunk, launches
+ * the level kernel and reads the counters back (one round trip per chunk).
+ * CP_ENGINE_GRAPH: the same schedule runs on the device -- a scheduler kernel
+ * and a persistent level kernel (warps claim boxes dynamically) inside a CUDA
+ * graph WHILE loop -- so a whole refinement is one graph launch; `block`
+ * (64, 128, 256, 512, 1024; 0 = tuned) and boxes_per_thread select the
+ * kernel shape.  Both engines produce identical reports. */
+typedef enum cp_engine { CP_ENGINE_LEVELS = 0, CP_ENGINE_GRAPH = 1 } cp_engine;
 
 typedef struct cp_refine_report {
     int64_t evaluated;       /* boxes evaluated */
@@ -251,10 +262,18 @@ cp_status cp_reference_criticals(cp_prover* p, int family, double la_lb, double 
 cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* opts, const double* lo, const double* hi,
                                const uint8_t* depth, size_t n, cp_refine_report* report);
 
+/* Diagnostics: the library's directed division (Newton reciprocal + exact
+ * FMA remainders, used for every interval division in place of the
+ * reference's __ddiv_rd/__ddiv_ru, interval.cuh:261-310) next to those
+ * intrinsics.  a, b: n device doubles; out: 4n device doubles per element
+ * (library RD, library RU, __ddiv_rd, __ddiv_ru).  Asynchronous. */
+cp_status cp_div_check(const double* a, const double* b, size_t n, double* out, void* stream);
+
 /* Diagnostics: measured peak throughput (operations per second, whole device)
  * of the FP64 primitives the criteria use, each run alone with full occupancy
  * and independent chains: rates[0] DFMA, [1] __dadd_rd, [2] __dmul_rd,
- * [3] __ddiv_rd, [4] asin (CUDA libm), [5] FFMA (FP32).  Synchronous. */
+ * [3] __ddiv_rd, [4] asin (CUDA libm), [5] FFMA (FP32), [6] the library's
+ * directed division (cp_div_check).  Synchronous. */
 cp_status cp_measure_primitives(int device, double* rates);
 
 /* ---------------------------------------------------------------- autotuning
@@ -266,6 +285,12 @@ cp_status cp_measure_primitives(int device, double* rates);
  * chosen variant in *best. */
 #define CP_LEVEL_VARIANTS 4
 cp_status cp_autotune(cp_prover* p, const cp_refine_opts* opts, int* best, double* ms);
+
+/* Graph engine autotuner: times opts' refinement (after one warm-up run) for
+ * every block size {64, 128, 256, 512, 1024} x boxes per thread {1, 2, 4, 8}
+ * and keeps the fastest for (family, precision).  ms: NULL or 20 doubles
+ * (row = block size, column = boxes per thread). */
+cp_status cp_autotune_graph(cp_prover* p, const cp_refine_opts* opts, int* block, int* boxes_per_thread, double* ms);
 
 /* Selects a level-kernel variant explicitly (0 .. CP_LEVEL_VARIANTS-1). */
 cp_status cp_set_level_variant(cp_prover* p, int family, int precision, int variant);
