@@ -47,7 +47,9 @@ def parse():
     ap.add_argument("--families", default="0,1,2,3,4,5", help="comma list (profiling runs)")
     ap.add_argument("--seed-res", type=int, default=64, help="lattice subdivisions per axis of the seed")
     ap.add_argument("--level-capacity", type=int, default=1 << 25, help="boxes per worklist level buffer")
-    ap.add_argument("--no-autotune", action="store_true", help="default kernel variants, FP64 (profiling runs)")
+    ap.add_argument("--no-autotune", action="store_true", help="default kernel shapes, FP64 (profiling runs)")
+    ap.add_argument("--no-learned", action="store_true", help="no proposal networks (reference criterion order)")
+    ap.add_argument("--no-proof", action="store_true", help="skip the full-domain proof leg")
     return ap.parse_args()
 
 
@@ -149,40 +151,108 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- workload
-def seed_opts(family, precision, depth):
+def seed_opts(family, form, depth):
+    """Refinement options of one family in a form: {"precision", "engine", "learned_order"}."""
     import circlepacking_b200 as cp
 
-    return dict(precision=precision, policy=cp.SPLIT_UNIFORM, max_depth=depth,
+    return dict(precision=form["precision"], policy=cp.SPLIT_UNIFORM, max_depth=depth,
                 seed_sizes=[SEED_RES] * DIMS[family], seed_lambda=(cp.LAMBDA_MIN, cp.LAMBDA_MAX),
-                level_capacity=LEVEL_CAP)
+                level_capacity=LEVEL_CAP, engine=form["engine"], learned_order=form.get("learned_order", False))
 
 
-def run_step(prover, precision, depth):
-    """One step over all families; precision: a cp precision or a per-family dict."""
-    reps = []
-    for f in FAMILIES:
-        prec = precision[f] if isinstance(precision, dict) else precision
-        reps.append(prover.refine(f, **seed_opts(f, prec, depth)))
-    return reps
+def run_step(prover, forms, depth):
+    """One step: the refinement of every family in its form."""
+    return [prover.refine(f, **seed_opts(f, forms[f], depth)) for f in FAMILIES]
 
 
-def autotune(prover, cp):
-    """Per family: the fastest level-kernel variant for each precision on a
-    calibration refinement (32^dims seed, one level), then the faster precision.
-    Both precisions give identical verdicts, so the choice is speed only."""
-    chosen, table = {}, {}
+def autotune(prover, cp, learned: bool):
+    """Per family, outside the timed region: the fastest form on a calibration
+    refinement (32^dims seed, one level) among the device-driven graph engine
+    (block size x boxes per thread) and the host-driven level loop (register
+    variants), each in FP64 and with the FP32 pre-pass, then (with `learned`)
+    whether the trained network's criterion order is faster still.  Every
+    candidate gives identical verdicts, so the choice is speed only."""
+    forms, table = {}, {}
     for f in FAMILIES:
         calib = dict(policy=cp.SPLIT_UNIFORM, max_depth=1, seed_sizes=[32] * DIMS[f])
-        t = {}
+        cands = []
         for prec in (cp.FP64, cp.FP32_PREFILTER):
+            blk, bpt, ms = prover.autotune_graph(f, precision=prec, **calib)
+            cands.append((min(min(r) for r in ms), prec, cp.ENGINE_GRAPH, {"block": blk, "boxes_per_thread": bpt}))
             v, ms = prover.autotune(f, precision=prec, **calib)
-            t[prec] = (min(ms), v, ms)
-        best = min(t, key=lambda k: t[k][0])
-        chosen[f] = best
-        table[cp.FAMILIES[f]] = {"precision": "fp64" if best == cp.FP64 else "fp32-prefilter",
-                                 "variant": t[best][1],
-                                 "calib_ms": {"fp64": t[cp.FP64][2], "fp32-prefilter": t[cp.FP32_PREFILTER][2]}}
-    return chosen, table
+            cands.append((min(ms), prec, cp.ENGINE_LEVELS, {"variant": v}))
+            prover.set_level_variant(f, prec, v)
+        ms, prec, eng, shape = min(cands, key=lambda c: c[0])
+        form = {"precision": prec, "engine": eng, "learned_order": False}
+        entry = {"precision": "fp64" if prec == cp.FP64 else "fp32-prefilter",
+                 "engine": "graph" if eng == cp.ENGINE_GRAPH else "levels", **shape, "calib_ms": ms,
+                 "candidates_ms": {f"{'fp64' if c[1] == cp.FP64 else 'fp32'}-{'graph' if c[2] else 'levels'}": c[0]
+                                   for c in cands}}
+        if learned and cp.N_CRITERIA[f] > 1:
+            kw = dict(calib, precision=prec, engine=eng)
+            base = min(prover.refine(f, **kw)["device_ms"] for _ in range(3))
+            lrn = min(prover.refine(f, learned_order=True, **kw)["device_ms"] for _ in range(3))
+            entry["calib_ms_learned_order"] = lrn
+            entry["calib_ms_reference_order"] = base
+            if lrn < base:
+                form["learned_order"] = True
+        entry["learned_order"] = form["learned_order"]
+        forms[f], table[cp.FAMILIES[f]] = form, entry
+    return forms, table
+
+
+def train_models(prover, cp, depth):
+    """The proposal network of every family with more than one criterion, trained
+    on the GPU on records of its own refinement (outside the timed region)."""
+    out = {}
+    for f in FAMILIES:
+        if cp.N_CRITERIA[f] < 2:
+            continue
+        t0 = time.perf_counter()
+        n = prover.model_collect(f, 1 << 21, sample_stride=8, policy=cp.SPLIT_UNIFORM, max_depth=depth,
+                                 seed_sizes=[32] * DIMS[f], level_capacity=LEVEL_CAP)
+        losses = prover.model_train(f, epochs=20, batch=4096, lr=1e-3, seed=1)
+        out[cp.FAMILIES[f]] = {"records": n, "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+                               "seconds": time.perf_counter() - t0}
+    return out
+
+
+PROOF_SEED = (64, 32, 32, 8)
+PROOF_DEPTH = 24
+PROOF_FAMILIES = (1, 3, 5)
+
+
+def proof_leg(prover, cp, forms, families):
+    """Full-domain proofs: the family's whole domain (lambda in [0.5, 0.99], the
+    dependent radius ranges) from a 64 x 32 x 32 (x 8) lattice seed, not-proved
+    boxes bisected in lambda only -- the reference's own refinement rule
+    (run_kernel.cuh:110-127) -- down to depth 24.  A family is proved when no box
+    is left unresolved.  Both forms evaluate the same tree of boxes, so their
+    verdict counts must be identical; the best form runs it as one graph launch."""
+    out = []
+    for f in families:
+        kw = dict(policy=cp.SPLIT_LAMBDA, max_depth=PROOF_DEPTH, seed_sizes=list(PROOF_SEED[:DIMS[f]]),
+                  seed_lambda=(cp.LAMBDA_MIN, cp.LAMBDA_MAX), level_capacity=1 << 23)
+        best_kw = dict(kw, precision=forms[f]["precision"], engine=cp.ENGINE_GRAPH,
+                       learned_order=forms[f].get("learned_order", False))
+        # the graph engine suits the proof's many small chunks; shape as tuned
+        plain_kw = dict(kw, precision=cp.FP64, engine=cp.ENGINE_LEVELS)
+        prover.refine(f, **best_kw)  # warm-up (graph build)
+        t0 = time.perf_counter()
+        b = prover.refine(f, **best_kw)
+        tb = time.perf_counter() - t0
+        prover.set_level_variant(f, cp.FP64, 0)
+        prover.refine(f, **plain_kw)
+        t0 = time.perf_counter()
+        p = prover.refine(f, **plain_kw)
+        tp = time.perf_counter() - t0
+        same = all(b[k] == p[k] for k in ("evaluated", "verdicts", "unresolved", "clipped", "per_depth"))
+        out.append({"family": cp.FAMILIES[f], "proved": b["unresolved"] == 0 and p["unresolved"] == 0,
+                    "boxes": b["evaluated"], "max_depth": len(b["per_depth"]) - 1,
+                    "best_wall_ms": tb * 1e3, "best_device_ms": b["device_ms"],
+                    "plain_wall_ms": tp * 1e3, "plain_device_ms": p["device_ms"],
+                    "plain_launches": p["launches"], "verdicts_identical": same})
+    return out
 
 
 def seed_boxes_host(family):
@@ -220,23 +290,26 @@ def roofline_work():
     return counts
 
 
-def roofline_of(cp, device, reps_plain) -> dict:
-    """Roofline of the FP64 level kernel: DFMA-equivalent work per box (each
-    primitive weighted by the measured DFMA rate over its own measured rate)
-    against the measured DFMA peak."""
+def roofline_of(cp, device, reps, ms_step) -> dict:
+    """Roofline of the FP64 criterion evaluation: DFMA-equivalent work per box
+    (each primitive of the reference's evaluation path, counted by the CPU
+    oracle, weighted by the measured DFMA rate over that primitive's measured
+    rate -- the library's own directed division for divisions) against the
+    measured DFMA peak, over the device time of the timed step."""
     rates = cp.measure_primitives(device)
     counts = roofline_work()
     work = 0.0
-    for f, r in zip(FAMILIES, reps_plain):
+    for f, r in zip(FAMILIES, reps):
         c = counts[f]
         per_box = (c["add"] * rates["dfma"] / rates["dadd_rd"] + c["mul"] * rates["dfma"] / rates["dmul_rd"]
-                   + c["div"] * rates["dfma"] / rates["ddiv_rd"] + c["asin"] * rates["dfma"] / rates["asin"]) / c["boxes"]
+                   + c["div"] * rates["dfma"] / rates["div_rd_lib"] + c["asin"] * rates["dfma"] / rates["asin"]
+                   ) / c["boxes"]
         work += r["evaluated"] * per_box
-    kernel_ms = sum(r["device_ms"] for r in reps_plain)
+    kernel_ms = sum(r["device_ms"] for r in reps)
     achieved = 2.0 * work / (kernel_ms / 1e3) / 1e12
     peak = 2.0 * rates["dfma"] / 1e12
     return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "k_level<family, fp64> (per-box FP64 criteria + split)",
+            "traffic": None, "kernel": "k_level_persist<family, fp64, block> (per-box FP64 criteria + split)",
             "work_model": "per box: CPU-oracle-counted add/mul/div/asin of the reference's evaluation path on the "
                           "seed lattices, each weighted by measured DFMA rate / primitive rate; peak = measured DFMA",
             "peaks_measured_tops": {k: v / 1e12 for k, v in rates.items()}, "peak_source": "measured in-process",
@@ -307,33 +380,37 @@ def main():
     torch.cuda.set_device(local)
     prover = cp.Prover(local)
     stream = prover.stream
-    FP64, PRE = cp.FP64, cp.FP32_PREFILTER
+    FP64 = cp.FP64
+    plain_forms = {f: {"precision": FP64, "engine": cp.ENGINE_LEVELS} for f in FAMILIES}
 
-    # ---- autotune (outside the timed region): kernel variant and precision per family
+    # ---- outside the timed region: proposal networks, kernel shapes, precisions
+    models = None
     if args.no_autotune:
-        chosen = {f: FP64 for f in FAMILIES}
-        tuning = {cp.FAMILIES[f]: {"precision": "fp64", "variant": 0} for f in FAMILIES}
+        forms = {f: {"precision": FP64, "engine": cp.ENGINE_GRAPH} for f in FAMILIES}
+        tuning = {cp.FAMILIES[f]: {"precision": "fp64", "engine": "graph"} for f in FAMILIES}
     else:
-        chosen, tuning = autotune(prover, cp)
+        if not args.no_learned:
+            models = train_models(prover, cp, args.depth)
+        forms, tuning = autotune(prover, cp, learned=not args.no_learned)
+
+    tuned_variant = {f: tuning[cp.FAMILIES[f]].get("variant", 1) for f in FAMILIES}
 
     def use_plain(on):
-        # the plain arm: FP64 with the untuned default kernel variant
+        # the plain arm: FP64, host-driven level loop, untuned kernel variant 0
         for f in FAMILIES:
-            if on:
-                prover.set_level_variant(f, FP64, 0)
-            elif tuning[cp.FAMILIES[f]]["precision"] == "fp64":
-                prover.set_level_variant(f, FP64, tuning[cp.FAMILIES[f]]["variant"])
+            prover.set_level_variant(f, FP64, 0 if on else tuned_variant[f])
 
     # ---- warm-up (also the verdict-identity check between the two forms)
     for _ in range(max(args.warmup, 3)):
-        best = run_step(prover, chosen, args.depth)
+        best = run_step(prover, forms, args.depth)
     use_plain(True)
-    plain = run_step(prover, FP64, args.depth)
+    plain = run_step(prover, plain_forms, args.depth)
     use_plain(False)
-    identical = all(b["verdicts"] == p["verdicts"] and b["unresolved"] == p["unresolved"] for b, p in zip(best, plain))
+    identical = all(b["verdicts"] == p["verdicts"] and b["unresolved"] == p["unresolved"]
+                    and b["per_depth"] == p["per_depth"] for b, p in zip(best, plain))
 
-    # ---- timed: best form, K steps on the prover's stream
-    def timed(precision):
+    # ---- timed: K steps on the prover's stream
+    def timed(fm):
         barrier(world)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -341,7 +418,7 @@ def main():
         e0.record(stream)
         reps = []
         for _ in range(args.steps):
-            reps = run_step(prover, precision, args.depth)
+            reps = run_step(prover, fm, args.depth)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
@@ -349,14 +426,19 @@ def main():
         return max_over_ranks(world, ms), reps
 
     with ClockSampler(local) as clk:
-        ms_best, reps_best = timed(chosen)
+        ms_best, reps_best = timed(forms)
     use_plain(True)
-    ms_plain, reps_plain = timed(FP64)
+    ms_plain, reps_plain = timed(plain_forms)
     use_plain(False)
     boxes_step = sum(r["evaluated"] for r in reps_best)
     value = sum_over_ranks(world, boxes_step) / (ms_best / 1e3)
     plain_value = sum_over_ranks(world, sum(r["evaluated"] for r in reps_plain)) / (ms_plain / 1e3)
-    launches_step = sum(r["launches"] + 2 for r in reps_best)  # level kernels + slab-bound + seed kernels
+    # kernels per step: the graph engine's chunk launches (+ scheduler, + inference
+    # with a learned order), the seed and slab-bound kernels
+    launches_step = sum(r["launches"] * ((3 if forms[f].get("learned_order") else 2)
+                                         if forms[f]["engine"] == cp.ENGINE_GRAPH else
+                                         (2 if forms[f].get("learned_order") else 1)) + 2
+                        for f, r in zip(FAMILIES, reps_best))
 
     # ---- e2e: the host-buffer C-ABI call (seed boxes from pinned host memory)
     e2e = None
@@ -370,7 +452,7 @@ def main():
             for f in FAMILIES:
                 lo, hi, dp = seeds[f]
                 r = prover.refine_boxes(f, lo.numpy(), hi.numpy(), depth=dp.numpy(),
-                                        **{k: v for k, v in seed_opts(f, chosen[f], args.depth).items()
+                                        **{k: v for k, v in seed_opts(f, forms[f], args.depth).items()
                                            if k not in ("seed_sizes", "seed_lambda")})
                 tot += r["evaluated"]
             return tot
@@ -386,10 +468,14 @@ def main():
         dt = max_over_ranks(world, (time.perf_counter() - t0) / args.steps)
         e2e = {"value": sum_over_ranks(world, tot / args.steps) / dt, "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3,
-               "call": "cp_refine_boxes_host per family (host seed boxes, report back)"}
+               "call": "cp_refine_boxes_host per family (host seed boxes, report back), best form"}
 
-    # ---- roofline of the FP64 criterion kernel (plain run)
-    roofline = None if args.no_roofline else roofline_of(cp, local, reps_plain)
+    # ---- full-domain proofs of the families that lambda-only refinement closes
+    proofs = None if args.no_proof else proof_leg(prover, cp, forms, [f for f in PROOF_FAMILIES if f in FAMILIES])
+    use_plain(False)
+
+    # ---- roofline of the FP64 criterion kernel (best form)
+    roofline = None if args.no_roofline else roofline_of(cp, local, reps_best, ms_best)
     cpu = cpu_baseline(args.cpu_seconds) if (rank == 0 and not args.no_cpu) else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -397,15 +483,22 @@ def main():
         "data": "synthetic",
         "config": {"workload": f"config-2 box set: 64^dims lattice seed per family over lambda [0.5,0.99], "
                                f"not-proved boxes bisected on all axes, {args.depth} levels, six families",
-                   "precision": "per family, autotuned: fp64 or fp32 enclosure pre-pass + fp64 (identical verdicts)",
-                   "autotune": tuning, "boxes_per_step": boxes_step,
+                   "form": "per family, autotuned: graph engine (block size x boxes per thread) or host-driven "
+                           "level loop (register variant), fp64 or fp32 pre-pass + fp64, learned criterion order "
+                           "when faster (identical verdicts)",
+                   "autotune": tuning, "models": models, "boxes_per_step": boxes_step,
                    "l2": "worklists of several GB per level (inputs > L2)", "parallelism": f"replicas x{world}"},
-        "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain},
+        "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain,
+                       "form": "fp64, host-driven level loop, kernel variant 0, reference criterion order"},
         "verdicts_identical": identical,
         "fp32_decided_fraction": sum(r["fp32_decided"] for r in reps_best) / max(1, boxes_step),
+        "criteria_per_box": {"best": sum(r["handles_evaluated"] for r in reps_best) / max(1, boxes_step),
+                             "plain": sum(r["handles_evaluated"] for r in reps_plain) /
+                             max(1, sum(r["evaluated"] for r in reps_plain))},
         "per_family": [{"family": cp.FAMILIES[f], "evaluated": r["evaluated"], "verdicts": r["verdicts"],
-                        "unresolved": r["unresolved"], "fp32_decided": r["fp32_decided"]}
+                        "unresolved": r["unresolved"], "fp32_decided": r["fp32_decided"], "device_ms": r["device_ms"]}
                        for f, r in zip(FAMILIES, reps_best)],
+        "full_domain_proofs": proofs,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
         "gpu_launches": launches_step * args.steps,
     }

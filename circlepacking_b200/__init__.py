@@ -246,9 +246,10 @@ def _declare_handle(L):
 def measure_primitives(device: int = 0) -> dict:
     L = lib()
     _declare_handle(L)
-    rates = np.zeros(7, np.float64)
+    rates = np.zeros(8, np.float64)
     _check(L.cp_measure_primitives(device, rates.ctypes.data), "cp_measure_primitives")
-    return dict(zip(("dfma", "dadd_rd", "dmul_rd", "ddiv_rd", "asin", "ffma", "div_rd_lib"), rates.tolist()))
+    return dict(zip(("dfma", "dadd_rd", "dmul_rd", "ddiv_rd", "asin", "ffma", "div_rd_lib", "div_rd_f32seed"),
+                    rates.tolist()))
 
 
 def div_check(a, b):

@@ -86,18 +86,19 @@ __device__ __forceinline__ double asin_ru(double x) {
 }
 
 // ------------------------------------------------------------------ directed division
-// a / b rounded toward -inf (DOWN) or +inf, bit-identical to __ddiv_rd /
-// __ddiv_ru.  Method (Markstein's FMA division, certified by exact remainders):
-//   y  ~ 1/b       hardware reciprocal approximation + two Newton steps
-//   q  = RN-ish(a/b)  q0 = a*y, refined once with the remainder a - q0*b
-//   the sign of t - c for the true quotient t = a/b and a candidate c is the
-//   sign of (a - c*b) / b; a - c*b is computed by one FMA and, for operands
-//   with |a|, |b| in [2^-500, 2^500], its rounded value has the exact sign
-//   (the exact difference is a multiple of 2^-606 or zero, far above the
-//   underflow threshold).  With q and its neighbour n in the direction of t,
-//   t in [q, n] (or [n, q]) is certified, which fixes both directed results.
-// Operands outside that range, and the (not expected) case where the
-// candidate is more than one unit in the last place away, use the intrinsic.
+// a / b rounded down / up, bit-identical to __ddiv_rd / __ddiv_ru.  Method:
+// Markstein's FMA division with the rounding direction read off an exact
+// remainder.  For |a|, |b| in [2^-500, 2^500]:
+//   y0 = rcp.approx(b), e = 1 - b*y0 (one FMA); if |e| >= 2^-18 the intrinsic
+//        is used instead.  y = y0 + y0*e then has |1 - b*y| <= e^2 + 2^-52.
+//   q0 = a*y;  q = q0 + (a - q0*b)*y   (two FMAs): |q - a/b| stays below half
+//        an ulp of q plus ~2^-72 |a/b|, so q is a faithful quotient.
+//   r  = a - q*b (one FMA): the exact difference is 0 or a multiple of
+//        ~2^-605, so its rounded value has the exact sign.  r = 0: a/b = q;
+//        otherwise a/b lies strictly between q and its neighbour on the side
+//        of sign(r)*sign(b), which fixes both directed results.
+// Operands outside the range (zeros, subnormals, infinities, NaN, extreme
+// exponents) use the intrinsics.
 __device__ __forceinline__ bool div_in_range(double a, double b) {
     const unsigned ea = ((unsigned)__double2hiint(a) >> 20) & 0x7ffu;
     const unsigned eb = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
@@ -112,30 +113,33 @@ __device__ __forceinline__ double next_down(double q) {
     const long long b = __double_as_longlong(q);
     return __longlong_as_double(q > 0.0 ? b - 1 : b + 1);
 }
-template <bool UP>
-__device__ __forceinline__ double div_dir(double a, double b) {
-    if (!div_in_range(a, b)) return UP ? __ddiv_ru(a, b) : __ddiv_rd(a, b);
+// Reciprocal seed: 0 = the FP64 approximation (rcp.approx.ftz.f64), 1 = the
+// FP32 reciprocal of b rounded to float (valid for |b| within float range).
+template <int SEED>
+__device__ __forceinline__ double rcp_seed(double b) {
     double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
-    double e = __fma_rn(-b, y, 1.0);
+    if (SEED == 0) {
+        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    } else {
+        float yf;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(__double2float_rn(b)));
+        y = (double)yf;
+    }
+    return y;
+}
+template <bool UP, int SEED = 0>
+__device__ __forceinline__ double div_dir(double a, double b) {
+    double y = rcp_seed<SEED>(b);
+    const double e = __fma_rn(-b, y, 1.0);
+    if (!div_in_range(a, b) || !(fabs(e) < 3.814697265625e-06)) return UP ? __ddiv_ru(a, b) : __ddiv_rd(a, b);
     y = __fma_rn(y, e, y);
-    e = __fma_rn(-b, y, 1.0);
-    if (!(fabs(e) < 1e-6)) return UP ? __ddiv_ru(a, b) : __ddiv_rd(a, b);  // reciprocal not close: no certificate
-    y = __fma_rn(y, e, y);
-    double q = __dmul_rn(a, y);
-    q = __fma_rn(__fma_rn(-q, b, a), y, q);
+    const double q0 = __dmul_rn(a, y);
+    const double q = __fma_rn(__fma_rn(-q0, b, a), y, q0);
     const double r = __fma_rn(-q, b, a);
-    if (r == 0.0) return q;  // exact quotient
-    const bool bneg = b < 0.0;
-    const bool above = (r > 0.0) != bneg;  // t > q
-    const double n = above ? next_up(q) : next_down(q);
-    const double rn = __fma_rn(-n, b, a);
-    if (rn == 0.0) return n;  // t == n exactly
-    const bool n_beyond = above ? ((rn < 0.0) != bneg) : ((rn > 0.0) != bneg);  // t strictly between q and n
-    if (!n_beyond) return UP ? __ddiv_ru(a, b) : __ddiv_rd(a, b);
-    // t in (q, n) when above, else in (n, q)
-    if (UP) return above ? n : q;
-    return above ? q : n;
+    if (r == 0.0) return q;                     // exact quotient
+    const bool above = (r > 0.0) != (b < 0.0);  // a/b > q
+    if (UP) return above ? next_up(q) : q;
+    return above ? q : next_down(q);
 }
 __device__ __forceinline__ double div_rd(double a, double b) { return div_dir<false>(a, b); }
 __device__ __forceinline__ double div_ru(double a, double b) { return div_dir<true>(a, b); }

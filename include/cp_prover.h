@@ -273,7 +273,8 @@ cp_status cp_div_check(const double* a, const double* b, size_t n, double* out, 
  * of the FP64 primitives the criteria use, each run alone with full occupancy
  * and independent chains: rates[0] DFMA, [1] __dadd_rd, [2] __dmul_rd,
  * [3] __ddiv_rd, [4] asin (CUDA libm), [5] FFMA (FP32), [6] the library's
- * directed division (cp_div_check).  Synchronous. */
+ * directed division (cp_div_check), [7] the same seeded from the FP32
+ * reciprocal (rates holds 8 doubles).  Synchronous. */
 cp_status cp_measure_primitives(int device, double* rates);
 
 /* ---------------------------------------------------------------- autotuning
