@@ -31,6 +31,7 @@ FAMILIES = range(6)
 DIMS = (4, 3, 4, 4, 3, 4)
 SEED_RES = 64
 LEVEL_CAP = 1 << 25
+SHARD = (0.5, 0.9900000000000001)  # this rank's lambda piece (the whole domain on one GPU)
 
 
 def parse():
@@ -50,6 +51,9 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="default kernel shapes, FP64 (profiling runs)")
     ap.add_argument("--no-learned", action="store_true", help="no proposal networks (reference criterion order)")
     ap.add_argument("--no-proof", action="store_true", help="skip the full-domain proof leg")
+    ap.add_argument("--reference-proof", default="3",
+                    help="families (comma list, '' = none) whose full-domain proof also runs by the reference's own "
+                         "method: its lambda loop over its lattice sizes, on the plain FP64 kernel")
     return ap.parse_args()
 
 
@@ -156,7 +160,7 @@ def seed_opts(family, form, depth):
     import circlepacking_b200 as cp
 
     return dict(precision=form["precision"], policy=cp.SPLIT_UNIFORM, max_depth=depth,
-                seed_sizes=[SEED_RES] * DIMS[family], seed_lambda=(cp.LAMBDA_MIN, cp.LAMBDA_MAX),
+                seed_sizes=[SEED_RES] * DIMS[family], seed_lambda=SHARD,
                 level_capacity=LEVEL_CAP, engine=form["engine"], learned_order=form.get("learned_order", False))
 
 
@@ -222,7 +226,7 @@ PROOF_DEPTH = 24
 PROOF_FAMILIES = (1, 3, 5)
 
 
-def proof_leg(prover, cp, forms, families):
+def proof_leg(prover, cp, forms, families, world=1):
     """Full-domain proofs: the family's whole domain (lambda in [0.5, 0.99], the
     dependent radius ranges) from a 64 x 32 x 32 (x 8) lattice seed, not-proved
     boxes bisected in lambda only -- the reference's own refinement rule
@@ -232,7 +236,7 @@ def proof_leg(prover, cp, forms, families):
     out = []
     for f in families:
         kw = dict(policy=cp.SPLIT_LAMBDA, max_depth=PROOF_DEPTH, seed_sizes=list(PROOF_SEED[:DIMS[f]]),
-                  seed_lambda=(cp.LAMBDA_MIN, cp.LAMBDA_MAX), level_capacity=1 << 23)
+                  seed_lambda=SHARD, level_capacity=1 << 23)
         best_kw = dict(kw, precision=forms[f]["precision"], engine=cp.ENGINE_GRAPH,
                        learned_order=forms[f].get("learned_order", False))
         # the graph engine suits the proof's many small chunks; shape as tuned
@@ -247,11 +251,16 @@ def proof_leg(prover, cp, forms, families):
         p = prover.refine(f, **plain_kw)
         tp = time.perf_counter() - t0
         same = all(b[k] == p[k] for k in ("evaluated", "verdicts", "unresolved", "clipped", "per_depth"))
-        out.append({"family": cp.FAMILIES[f], "proved": b["unresolved"] == 0 and p["unresolved"] == 0,
-                    "boxes": b["evaluated"], "max_depth": len(b["per_depth"]) - 1,
-                    "best_wall_ms": tb * 1e3, "best_device_ms": b["device_ms"],
-                    "plain_wall_ms": tp * 1e3, "plain_device_ms": p["device_ms"],
-                    "plain_launches": p["launches"], "verdicts_identical": same})
+        # over all ranks' lambda pieces: counts summed, times the slowest rank's
+        unresolved = sum_over_ranks(world, b["unresolved"] + p["unresolved"])
+        out.append({"family": cp.FAMILIES[f], "proved": unresolved == 0,
+                    "boxes": int(sum_over_ranks(world, b["evaluated"])), "max_depth": len(b["per_depth"]) - 1,
+                    "best_wall_ms": max_over_ranks(world, tb * 1e3),
+                    "best_device_ms": max_over_ranks(world, b["device_ms"]),
+                    "plain_wall_ms": max_over_ranks(world, tp * 1e3),
+                    "plain_device_ms": max_over_ranks(world, p["device_ms"]),
+                    "plain_launches": p["launches"],
+                    "verdicts_identical": sum_over_ranks(world, 0 if same else 1) == 0})
     return out
 
 
@@ -263,8 +272,7 @@ def seed_boxes_host(family):
 
     total = SEED_RES ** DIMS[family]
     idx = torch.arange(total, device="cuda", dtype=torch.int64)
-    lo, hi, vis = cp.lattice_boxes(family, (cp.LAMBDA_MIN, cp.LAMBDA_MAX), [SEED_RES] * DIMS[family], idx,
-                                   visited=True)
+    lo, hi, vis = cp.lattice_boxes(family, SHARD, [SEED_RES] * DIMS[family], idx, visited=True)
     hlo = torch.empty(lo.shape, dtype=torch.float64, pin_memory=True)
     hhi = torch.empty(hi.shape, dtype=torch.float64, pin_memory=True)
     hdp = torch.empty(vis.shape, dtype=torch.uint8, pin_memory=True)
@@ -366,7 +374,7 @@ def main_reference(args, world, rank):
 
 def main():
     args = parse()
-    global FAMILIES, SEED_RES, LEVEL_CAP
+    global FAMILIES, SEED_RES, LEVEL_CAP, SHARD
     FAMILIES = [int(x) for x in args.families.split(",")]
     SEED_RES, LEVEL_CAP = args.seed_res, args.level_capacity
     world, rank, local = dist_init()
@@ -376,6 +384,10 @@ def main():
     import torch
 
     import circlepacking_b200 as cp
+
+    # lambda sharding: each rank refines its own piece of the domain from a full
+    # 64^dims seed (weak scaling); boxes are independent, so no data exchange
+    SHARD = cp.lambda_shard(rank, world)
 
     torch.cuda.set_device(local)
     prover = cp.Prover(local)
@@ -471,7 +483,24 @@ def main():
                "call": "cp_refine_boxes_host per family (host seed boxes, report back), best form"}
 
     # ---- full-domain proofs of the families that lambda-only refinement closes
-    proofs = None if args.no_proof else proof_leg(prover, cp, forms, [f for f in PROOF_FAMILIES if f in FAMILIES])
+    proofs = None if args.no_proof else proof_leg(prover, cp, forms, [f for f in PROOF_FAMILIES if f in FAMILIES], world)
+    if proofs is not None and args.reference_proof:
+        # the same proofs by the reference's own method (run_kernel.cuh:61-132 with
+        # the lattice sizes of its family kernels), timed on this GPU
+        for f in [int(x) for x in args.reference_proof.split(",")]:
+            if f not in FAMILIES or SHARD != (cp.LAMBDA_MIN, cp.LAMBDA_MAX):
+                continue
+            prover.set_level_variant(f, FP64, 0)
+            t0 = time.perf_counter()
+            ref = prover.prove_family_reference(f)
+            t_ref = time.perf_counter() - t0
+            for e in proofs:
+                if e["family"] == cp.FAMILIES[f]:
+                    e["reference_method"] = {"proved": ref["proved"], "wall_ms": t_ref * 1e3,
+                                             "device_ms": ref["device_ms"], "launches": ref["launches"],
+                                             "boxes": ref["boxes_evaluated"],
+                                             "lattice": list(cp.REFERENCE_SIZES[f][:DIMS[f]])}
+                    e["speedup_vs_reference_method"] = t_ref * 1e3 / e["best_wall_ms"]
     use_plain(False)
 
     # ---- roofline of the FP64 criterion kernel (best form)
@@ -487,7 +516,8 @@ def main():
                            "level loop (register variant), fp64 or fp32 pre-pass + fp64, learned criterion order "
                            "when faster (identical verdicts)",
                    "autotune": tuning, "models": models, "boxes_per_step": boxes_step,
-                   "l2": "worklists of several GB per level (inputs > L2)", "parallelism": f"replicas x{world}"},
+                   "l2": "worklists of several GB per level (inputs > L2)",
+                   "parallelism": f"lambda shards x{world} (each rank: 64^dims seed over its lambda piece)"},
         "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain,
                        "form": "fp64, host-driven level loop, kernel variant 0, reference criterion order"},
         "verdicts_identical": identical,

@@ -503,3 +503,45 @@ class _ModelMixin:
 
 for _name in ("model_collect", "model_records", "model_train", "model_params", "model_set_params", "model_predict"):
     setattr(Prover, _name, getattr(_ModelMixin, _name))
+
+
+# ---------------------------------------------------------------- multi-GPU sharding
+def lambda_shard(rank: int, world: int, lo: float = LAMBDA_MIN, hi: float = LAMBDA_MAX):
+    """The lambda sub-range of `rank` among `world` ranks: [lo, hi] cut into
+    `world` equal pieces; neighbouring ranks compute their shared boundary by the
+    same expression, so the pieces tile [lo, hi] exactly (no gap, no overlap
+    beyond the shared endpoint).  Boxes are independent, so ranks refine their
+    pieces with no data exchange; only the final counts are summed."""
+    if world < 1 or not (0 <= rank < world):
+        raise ValueError("rank must be in [0, world)")
+
+    def cut(k):
+        if k == 0:
+            return lo
+        if k == world:
+            return hi
+        return lo + (hi - lo) / world * k
+
+    return cut(rank), cut(rank + 1)
+
+
+def reduce_report(report: dict, group=None) -> dict:
+    """Sums a refinement report's counts over the ranks of a torch.distributed
+    group (any backend); times become the maximum over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    keys = ("evaluated", "unresolved", "clipped", "fp32_decided", "handles_evaluated")
+    v = torch.tensor([report[k] for k in keys] + list(report["verdicts"]), dtype=torch.float64)
+    t = torch.tensor([report["device_ms"], report["wall_ms"]], dtype=torch.float64)
+    if dist.get_backend(group) == "nccl":
+        v, t = v.cuda(), t.cuda()
+    dist.all_reduce(v, op=dist.ReduceOp.SUM, group=group)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    v, t = v.cpu().tolist(), t.cpu().tolist()
+    out = dict(report)
+    for i, k in enumerate(keys):
+        out[k] = int(v[i])
+    out["verdicts"] = [int(x) for x in v[len(keys):]]
+    out["device_ms"], out["wall_ms"] = t
+    return out
