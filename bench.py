@@ -510,7 +510,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_best, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"config-2 box set: 64^dims lattice seed per family over lambda [0.5,0.99], "
+        "config": {"workload": f"uniform-bisection box set: 64^dims lattice seed per family over lambda [0.5,0.99], "
                                f"not-proved boxes bisected on all axes, {args.depth} levels, six families",
                    "form": "per family, autotuned: graph engine (block size x boxes per thread) or host-driven "
                            "level loop (register variant), fp64 or fp32 pre-pass + fp64, learned criterion order "

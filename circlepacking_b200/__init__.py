@@ -182,7 +182,7 @@ def asin_pad(x):
 
 
 # ---------------------------------------------------------------- prover handle
-SPLIT_UNIFORM, SPLIT_LAMBDA, SPLIT_WIDEST, SPLIT_LEARNED = range(4)
+SPLIT_UNIFORM, SPLIT_LAMBDA, SPLIT_WIDEST, SPLIT_LEARNED, SPLIT_HYBRID = range(5)
 ENGINE_LEVELS, ENGINE_GRAPH = 0, 1
 GRAPH_BLOCKS, GRAPH_BPT = (64, 128, 256, 512, 1024), (1, 2, 4, 8)
 REFERENCE_SIZES = ((256, 256, 256, 64), (4096, 4096, 4096), (256, 256, 256, 64), (512, 256, 256, 64),
@@ -193,7 +193,7 @@ class RefineOpts(ctypes.Structure):
     _fields_ = [("family", ctypes.c_int32), ("precision", ctypes.c_int32), ("policy", ctypes.c_int32),
                 ("max_depth", ctypes.c_int32), ("seed_sizes", ctypes.c_int32 * 4), ("seed_lambda", ctypes.c_double * 2),
                 ("level_capacity", ctypes.c_int64), ("block", ctypes.c_int32), ("learned_order", ctypes.c_int32),
-                ("engine", ctypes.c_int32), ("boxes_per_thread", ctypes.c_int32)]
+                ("engine", ctypes.c_int32), ("boxes_per_thread", ctypes.c_int32), ("lambda_scale", ctypes.c_double)]
 
 
 class RefineReport(ctypes.Structure):
@@ -303,7 +303,8 @@ class Prover:
 
     @staticmethod
     def opts(family, precision=FP64, policy=SPLIT_UNIFORM, max_depth=2, seed_sizes=None, seed_lambda=None,
-             level_capacity=0, learned_order=False, engine=ENGINE_LEVELS, block=0, boxes_per_thread=0) -> RefineOpts:
+             level_capacity=0, learned_order=False, engine=ENGINE_LEVELS, block=0, boxes_per_thread=0,
+             lambda_scale=0.0) -> RefineOpts:
         o = RefineOpts()
         o.family, o.precision, o.policy, o.max_depth = family, precision, policy, max_depth
         ss = list(seed_sizes or [64] * DIMS[family]) + [1] * 4
@@ -316,6 +317,7 @@ class Prover:
         o.learned_order = int(bool(learned_order))
         o.engine = engine
         o.boxes_per_thread = boxes_per_thread
+        o.lambda_scale = lambda_scale
         return o
 
     def autotune(self, family, **kw):

@@ -226,6 +226,9 @@ unsigned grid_of(K kernel, int block) {
     return (unsigned)(sms * per_sm);
 }
 
+constexpr double kDefaultLambdaScale = 4e-3;
+double lambda_scale_of(const cp_refine_opts& o) { return o.lambda_scale > 0.0 ? o.lambda_scale : kDefaultLambdaScale; }
+
 double now_ms() {
     using namespace std::chrono;
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
@@ -263,7 +266,7 @@ struct cp_prover {
     DevSched* h_sched = nullptr;  // pinned mirror
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
-    unsigned long long graph_key[11] = {0};
+    unsigned long long graph_key[12] = {0};
     int graph_variant[6][2] = {{1, 1}, {1, 1}, {1, 1}, {1, 1}, {1, 1}, {1, 1}};  // block-size variant
     int graph_bpt[6][2] = {{2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}};      // boxes per thread
     int variant[6][2] = {{1, 1}, {0, 0}, {1, 1}, {1, 1}, {0, 0}, {1, 1}};  // level-kernel variant per family/precision
@@ -397,6 +400,7 @@ cp_status cp_engine_launch_level(int fam, int prec, int variant, const BoxList& 
     a.per_depth = counters + C_COUNT;
     a.tab = SingleTable{tab_t, tab_v, tab_n, tab_h};
     a.policy = policy == CP_SPLIT_LEARNED ? SPLIT_GIVEN : policy;
+    a.lambda_scale = kDefaultLambdaScale;
     a.max_depth = out ? max_depth : 0;
     a.axis_hint = nullptr;
     a.order_hint = nullptr;
@@ -442,6 +446,7 @@ cp_status cp_engine_eval_chunk(cp_prover* p, int fam, const cp_refine_opts& o, L
     a.per_depth = p->per_depth;
     a.tab = table_of(p);
     a.policy = o.policy == CP_SPLIT_LEARNED ? SPLIT_GIVEN : o.policy;
+    a.lambda_scale = lambda_scale_of(o);
     a.max_depth = out ? o.max_depth : 0;
     a.axis_hint = axis_hint;
     a.order_hint = order_hint;
@@ -578,6 +583,7 @@ cp_status build_graph(cp_prover* p, const cp_refine_opts& o, int variant, int bp
         pa.per_depth = p->per_depth;
         pa.tab = table_of(p);
         pa.policy = o.policy == CP_SPLIT_LEARNED ? SPLIT_GIVEN : o.policy;
+        pa.lambda_scale = lambda_scale_of(o);
         pa.max_depth = o.max_depth;
         pa.bpt = bpt;
         pa.axis_hint = axis;
@@ -627,7 +633,10 @@ cp_status refine_graph(cp_prover* p, const cp_refine_opts& o, cp_refine_report* 
     CP_TRY(cuda_ok(cudaMemcpyAsync(p->d_levels, hl, sizeof(BoxList) * nlevels, cudaMemcpyHostToDevice, p->stream)));
     CP_TRY(cuda_ok(cudaMemcpyAsync(p->d_sched, &hs, sizeof(DevSched), cudaMemcpyHostToDevice, p->stream)));
     if (learned_axis || learned_order) CP_TRY(cp_model_reserve_hints(p, p->level_cap));
-    const unsigned long long key[11] = {(unsigned long long)fam + 1, (unsigned long long)prec, (unsigned long long)variant,
+    double ls = lambda_scale_of(o);
+    unsigned long long ls_bits;
+    std::memcpy(&ls_bits, &ls, 8);
+    const unsigned long long key[12] = {ls_bits, (unsigned long long)fam + 1, (unsigned long long)prec, (unsigned long long)variant,
                                         (unsigned long long)bpt, (unsigned long long)o.policy,
                                         (unsigned long long)o.max_depth,
                                         (unsigned long long)(learned_axis | (learned_order << 1)),
@@ -664,7 +673,8 @@ cp_status run_refinement(cp_prover* p, const cp_refine_opts& o, cp_refine_report
 cp_status check_opts(const cp_refine_opts* o) {
     if (!o || o->family < 0 || o->family > 5) return CP_ERR_INVALID;
     if (o->precision != CP_FP64 && o->precision != CP_FP32_PREFILTER) return CP_ERR_INVALID;
-    if (o->policy < CP_SPLIT_UNIFORM || o->policy > CP_SPLIT_LEARNED) return CP_ERR_INVALID;
+    if (o->policy < CP_SPLIT_UNIFORM || o->policy > CP_SPLIT_HYBRID) return CP_ERR_INVALID;
+    if (!(o->lambda_scale >= 0.0)) return CP_ERR_INVALID;
     if (o->max_depth < 0 || o->max_depth > 250) return CP_ERR_INVALID;
     if (o->engine != CP_ENGINE_LEVELS && o->engine != CP_ENGINE_GRAPH) return CP_ERR_INVALID;
     if (o->boxes_per_thread < 0 || o->boxes_per_thread > 8) return CP_ERR_INVALID;

@@ -21,6 +21,7 @@ struct PersistArgs {
     unsigned long long* per_depth;
     SingleTable tab;
     int policy, max_depth, bpt;
+    double lambda_scale;
     const uint8_t* axis_hint;   // per box of the job, indexed from job.begin
     const uint8_t* order_hint;
 };
@@ -42,6 +43,7 @@ __global__ void __launch_bounds__(BLOCK) __maxnreg__(graph_regs(BLOCK)) k_level_
     a.per_depth = pa.per_depth;
     a.tab = pa.tab;
     a.policy = pa.policy;
+    a.lambda_scale = pa.lambda_scale;
     a.max_depth = job.out_level >= 0 ? pa.max_depth : 0;
     a.axis_hint = pa.axis_hint;
     a.order_hint = pa.order_hint;

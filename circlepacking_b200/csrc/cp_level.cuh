@@ -42,6 +42,7 @@ struct LevelArgs {
     unsigned long long* per_depth;
     SingleTable tab;
     int policy, max_depth;
+    double lambda_scale;        // SPLIT_HYBRID
     const uint8_t* axis_hint;   // per input box (SPLIT_GIVEN), indexed from `begin`
     const uint8_t* order_hint;  // per input box criterion order, or null
 };
@@ -109,6 +110,8 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                     nchild = fanout(a.policy, D);
                     if (a.policy == SPLIT_WIDEST)
                         axis = widest_axis<D>(lo, hi);
+                    else if (a.policy == SPLIT_HYBRID)
+                        axis = hybrid_axis<D>(lo, hi, a.lambda_scale);
                     else if (a.policy == SPLIT_GIVEN)
                         axis = a.axis_hint ? (a.axis_hint[j] % D) : 0;
                 }

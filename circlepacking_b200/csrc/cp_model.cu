@@ -72,6 +72,13 @@ __device__ __forceinline__ float gelu(float x) {
     const float t = tanhf(kGeluC * (x + 0.044715f * x * x * x));
     return 0.5f * x * (1.0f + t);
 }
+// Inference GELU: the hardware tanh approximation (tanh.approx.f32, one MUFU
+// operation; maximum relative error about 2^-11), which is below BF16 resolution.
+__device__ __forceinline__ float gelu_fast(float x) {
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(kGeluC * (x + 0.044715f * x * x * x)));
+    return 0.5f * x * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_grad(float x) {
     const float t = tanhf(kGeluC * (x + 0.044715f * x * x * x));
     return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * 0.044715f * x * x);
@@ -88,6 +95,29 @@ __device__ __forceinline__ void box_features(const double* lo, const double* hi,
             const double w = fmax(hi[d] - lo[d], 1e-300);
             f[2 * d] = (float)((c - a) / rng * 2.0 - 1.0);
             f[2 * d + 1] = (float)(log2(w / rng) / 16.0 + 1.0);
+        } else {
+            f[2 * d] = 0.f;
+            f[2 * d + 1] = 0.f;
+        }
+    }
+    f[8] = (float)depth / 32.0f;
+#pragma unroll
+    for (int k = 9; k < 16; ++k) f[k] = 0.f;
+}
+
+// The same features in single precision (inference): widths stay above 2^-126
+// for every depth the engine reaches, so FP32 log2 loses nothing at BF16
+// resolution.
+template <int D>
+__device__ __forceinline__ void box_features_fast(const double* lo, const double* hi, int depth, float* f) {
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        if (d < D) {
+            const float a = d == 0 ? 0.5f : 0.0f, inv = d == 0 ? (1.0f / 0.49f) : 4.0f;
+            const float c = (float)(0.5 * (lo[d] + hi[d]));
+            const float w = fmaxf((float)(hi[d] - lo[d]) * inv, 1e-37f);
+            f[2 * d] = (c - a) * inv * 2.0f - 1.0f;
+            f[2 * d + 1] = __log2f(w) * (1.0f / 16.0f) + 1.0f;
         } else {
             f[2 * d] = 0.f;
             f[2 * d + 1] = 0.f;
@@ -125,6 +155,12 @@ struct Acts {
     uint32_t g1[4][4], g2[4][4];
 };
 
+template <bool FAST>
+__device__ __forceinline__ float act(float x) {
+    return FAST ? gelu_fast(x) : gelu(x);
+}
+
+template <bool FAST>
 __device__ __forceinline__ void forward16(const FwdSmem& s, const bf16* x, Acts& A) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const uint32_t ax[4] = {ld32(x + g * PK + 2 * t), ld32(x + (g + 8) * PK + 2 * t), ld32(x + g * PK + 2 * t + 8),
@@ -139,10 +175,10 @@ __device__ __forceinline__ void forward16(const FwdSmem& s, const bf16* x, Acts&
     }
 #pragma unroll
     for (int kt = 0; kt < 4; ++kt) {
-        A.g1[kt][0] = pack2(gelu(A.h1[2 * kt][0]), gelu(A.h1[2 * kt][1]));
-        A.g1[kt][1] = pack2(gelu(A.h1[2 * kt][2]), gelu(A.h1[2 * kt][3]));
-        A.g1[kt][2] = pack2(gelu(A.h1[2 * kt + 1][0]), gelu(A.h1[2 * kt + 1][1]));
-        A.g1[kt][3] = pack2(gelu(A.h1[2 * kt + 1][2]), gelu(A.h1[2 * kt + 1][3]));
+        A.g1[kt][0] = pack2(act<FAST>(A.h1[2 * kt][0]), act<FAST>(A.h1[2 * kt][1]));
+        A.g1[kt][1] = pack2(act<FAST>(A.h1[2 * kt][2]), act<FAST>(A.h1[2 * kt][3]));
+        A.g1[kt][2] = pack2(act<FAST>(A.h1[2 * kt + 1][0]), act<FAST>(A.h1[2 * kt + 1][1]));
+        A.g1[kt][3] = pack2(act<FAST>(A.h1[2 * kt + 1][2]), act<FAST>(A.h1[2 * kt + 1][3]));
     }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -157,10 +193,10 @@ __device__ __forceinline__ void forward16(const FwdSmem& s, const bf16* x, Acts&
     }
 #pragma unroll
     for (int kt = 0; kt < 4; ++kt) {
-        A.g2[kt][0] = pack2(gelu(A.h2[2 * kt][0]), gelu(A.h2[2 * kt][1]));
-        A.g2[kt][1] = pack2(gelu(A.h2[2 * kt][2]), gelu(A.h2[2 * kt][3]));
-        A.g2[kt][2] = pack2(gelu(A.h2[2 * kt + 1][0]), gelu(A.h2[2 * kt + 1][1]));
-        A.g2[kt][3] = pack2(gelu(A.h2[2 * kt + 1][2]), gelu(A.h2[2 * kt + 1][3]));
+        A.g2[kt][0] = pack2(act<FAST>(A.h2[2 * kt][0]), act<FAST>(A.h2[2 * kt][1]));
+        A.g2[kt][1] = pack2(act<FAST>(A.h2[2 * kt][2]), act<FAST>(A.h2[2 * kt][3]));
+        A.g2[kt][2] = pack2(act<FAST>(A.h2[2 * kt + 1][0]), act<FAST>(A.h2[2 * kt + 1][1]));
+        A.g2[kt][3] = pack2(act<FAST>(A.h2[2 * kt + 1][2]), act<FAST>(A.h2[2 * kt + 1][3]));
     }
     float acc[4] = {s.b3[2 * t], s.b3[2 * t + 1], s.b3[2 * t], s.b3[2 * t + 1]};
 #pragma unroll
@@ -232,7 +268,7 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_train_step(TrainArgs a) {
     __syncthreads();
 
     Acts A;
-    forward16(s.f, s.x[warp], A);
+    forward16<false>(s.f, s.x[warp], A);
     const int rw = kRowsPerWarp * warp;  // warp's first row within the block
     // stage G1, G2 transposed for the weight gradients
 #pragma unroll
@@ -543,7 +579,7 @@ __global__ void __launch_bounds__(128) k_infer(InferArgs a) {
                     hi[d] = a.in.hi[d * a.in.cap + i];
                 }
                 const int depth = a.in.depth[i];
-                box_features<D>(lo, hi, depth == 0xFF ? 0 : depth, f);
+                box_features_fast<D>(lo, hi, depth == 0xFF ? 0 : depth, f);
             } else {
 #pragma unroll
                 for (int k = 0; k < 16; ++k) f[k] = 0.f;
@@ -553,7 +589,7 @@ __global__ void __launch_bounds__(128) k_infer(InferArgs a) {
         }
         __syncwarp();
         Acts A;
-        forward16(s.f, s.x[warp], A);
+        forward16<true>(s.f, s.x[warp], A);
         s.z[warp][g * NO + 2 * t] = A.z[0];
         s.z[warp][g * NO + 2 * t + 1] = A.z[1];
         s.z[warp][(g + 8) * NO + 2 * t] = A.z[2];

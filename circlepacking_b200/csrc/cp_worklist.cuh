@@ -19,7 +19,8 @@ enum SplitPolicy : int {
     SPLIT_UNIFORM = 0,  // bisect every axis: 2^dims children
     SPLIT_LAMBDA = 1,   // bisect lambda only (the reference refines lambda only, run_kernel.cuh:110-127)
     SPLIT_WIDEST = 2,   // bisect the axis with the largest width relative to its scale
-    SPLIT_GIVEN = 3     // bisect the axis chosen per box by the learned model
+    SPLIT_GIVEN = 3,    // bisect the axis chosen per box by the learned model
+    SPLIT_HYBRID = 4    // lambda while wider than its target width, else the widest radius
 };
 
 // Single-placement bounds on a uniform lambda grid t_i = 0.5 + i*h, i = 0..n-1,
@@ -81,6 +82,24 @@ __device__ __forceinline__ int widest_axis(const double* lo, const double* hi) {
             ax = d;
         }
     }
+    return ax;
+}
+
+// Hybrid rule: the width lambda needs shrinks about like (1 - lambda)^2 toward
+// the top of the domain; above `scale * (1 - la.hi)^2` lambda is bisected,
+// below it the radius whose width is largest relative to the lane width.
+template <int D>
+__device__ __forceinline__ int hybrid_axis(const double* lo, const double* hi, double scale) {
+    const double lane = 1.0 - hi[0];
+    if (hi[0] - lo[0] > scale * lane * lane) return 0;
+    int ax = 1;
+    double best = hi[1] - lo[1];
+#pragma unroll
+    for (int d = 2; d < D; ++d)
+        if (hi[d] - lo[d] > best) {
+            best = hi[d] - lo[d];
+            ax = d;
+        }
     return ax;
 }
 

@@ -51,7 +51,7 @@ typedef enum cp_status {
     CP_ERR_NO_DEVICE = 10    /* no CUDA device, or the library's kernels cannot run on it */
 } cp_status;
 
-/* The six families (one reference kernel each, SURVEY order). */
+/* The six families (one reference kernel each, in the order the reference proves them, lane_packing.cu:32-37). */
 typedef enum cp_family {
     CP_START = 0,        /* start_configuration.cu:114-167 */
     CP_START_END_2D = 1, /* start_configuration.cu:190-215 */
@@ -166,7 +166,9 @@ typedef enum cp_split_policy {
     CP_SPLIT_UNIFORM = 0, /* bisect every axis (2^dims children) */
     CP_SPLIT_LAMBDA = 1,  /* bisect lambda only (the reference refines lambda only) */
     CP_SPLIT_WIDEST = 2,  /* bisect the axis with the largest relative width */
-    CP_SPLIT_LEARNED = 3  /* bisect the axis the learned model picks (cp_load_model) */
+    CP_SPLIT_LEARNED = 3, /* bisect the axis the learned model picks (trained or loaded model) */
+    CP_SPLIT_HYBRID = 4   /* bisect lambda while its width exceeds lambda_scale * (1 - lambda.hi)^2,
+                             else the radius widest relative to the lane width 1 - lambda.hi */
 } cp_split_policy;
 
 typedef struct cp_refine_opts {
@@ -181,6 +183,7 @@ typedef struct cp_refine_opts {
     int32_t learned_order;  /* 1 = learned criterion order (needs a trained or loaded model) */
     int32_t engine;         /* cp_engine: host-driven level loop or one CUDA graph launch */
     int32_t boxes_per_thread; /* graph engine: boxes a warp lane takes per claim (1..8); 0 = tuned */
+    double lambda_scale;    /* CP_SPLIT_HYBRID: lambda target width scale; 0 = 4e-3 */
 } cp_refine_opts;
 
 /* Refinement engines.  CP_ENGINE_LEVELS: the host picks each chunk, launches

@@ -25,7 +25,7 @@ def _same(a, b):
 
 
 @pytest.mark.parametrize("family", range(6))
-@pytest.mark.parametrize("policy,depth", [(0, 2), (1, 6), (2, 7)])
+@pytest.mark.parametrize("policy,depth", [(0, 2), (1, 6), (2, 7), (4, 9)])
 def test_graph_matches_level_loop(cp, prover, family, policy, depth):
     dims = boxgen.DIMS[family]
     kw = dict(policy=policy, max_depth=depth, seed_sizes=[16, 8, 8, 4][:dims], level_capacity=1 << 20)
