@@ -11,7 +11,7 @@
 //
 // Features of a box (computed in FP64, rounded to BF16): per axis d < dims the
 // centre mapped to [-1, 1] over the axis' nominal range and
-// log2(width / range) / 16 + 1; then depth / 32.  Ranges: lambda [0.5, 0.99],
+// log2(max(width / range, 2^-64)) / 16 + 1; then depth / 32.  Ranges: lambda [0.5, 0.99],
 // radii [0, 0.25].
 //
 // Training records come from the prover's own refinement (cp_model_collect):
@@ -92,9 +92,9 @@ __device__ __forceinline__ void box_features(const double* lo, const double* hi,
         if (d < D) {
             const double a = d == 0 ? 0.5 : 0.0, rng = d == 0 ? 0.49 : 0.25;
             const double c = 0.5 * (lo[d] + hi[d]);
-            const double w = fmax(hi[d] - lo[d], 1e-300);
+            const double w = fmax((hi[d] - lo[d]) / rng, 5.421010862427522e-20);  // 2^-64
             f[2 * d] = (float)((c - a) / rng * 2.0 - 1.0);
-            f[2 * d + 1] = (float)(log2(w / rng) / 16.0 + 1.0);
+            f[2 * d + 1] = (float)(log2(w) / 16.0 + 1.0);
         } else {
             f[2 * d] = 0.f;
             f[2 * d + 1] = 0.f;
@@ -105,8 +105,8 @@ __device__ __forceinline__ void box_features(const double* lo, const double* hi,
     for (int k = 9; k < 16; ++k) f[k] = 0.f;
 }
 
-// The same features in single precision (inference): widths stay above 2^-126
-// for every depth the engine reaches, so FP32 log2 loses nothing at BF16
+// The same features in single precision (inference): the relative width is
+// clamped at 2^-64, far inside FP32 range, so FP32 log2 loses nothing at BF16
 // resolution.
 template <int D>
 __device__ __forceinline__ void box_features_fast(const double* lo, const double* hi, int depth, float* f) {
@@ -115,7 +115,7 @@ __device__ __forceinline__ void box_features_fast(const double* lo, const double
         if (d < D) {
             const float a = d == 0 ? 0.5f : 0.0f, inv = d == 0 ? (1.0f / 0.49f) : 4.0f;
             const float c = (float)(0.5 * (lo[d] + hi[d]));
-            const float w = fmaxf((float)(hi[d] - lo[d]) * inv, 1e-37f);
+            const float w = fmaxf((float)(hi[d] - lo[d]) * inv, 5.421010862427522e-20f);  // 2^-64
             f[2 * d] = (c - a) * inv * 2.0f - 1.0f;
             f[2 * d + 1] = __log2f(w) * (1.0f / 16.0f) + 1.0f;
         } else {

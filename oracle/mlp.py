@@ -10,8 +10,8 @@ and activations as GEMM operands with FP32 (here: FP64) accumulation.
   logits 0..3  failure of sub-criterion k (binary cross-entropy, k < K)
   logits 4..7  split axis (softmax cross-entropy over the family's axes)
 Features of a box (lo, hi per axis, depth): per axis d < dims the centre mapped
-to [-1, 1] over the axis' nominal range and log2(width / range) / 16 + 1; then
-depth / 32.  Axis ranges: lambda [0.5, 0.99], radii [0, 0.25].
+to [-1, 1] over the axis' nominal range and log2(max(width / range, 2^-64)) / 16
++ 1; then depth / 32.  Axis ranges: lambda [0.5, 0.99], radii [0, 0.25].
 """
 from __future__ import annotations
 
@@ -52,9 +52,9 @@ def features(family: int, lo: np.ndarray, hi: np.ndarray, depth: np.ndarray) -> 
         a, b = AXIS_RANGE[d]
         rng = b - a
         c = 0.5 * (lo[d] + hi[d])
-        w = np.maximum(hi[d] - lo[d], 1e-300)
+        w = np.maximum((hi[d] - lo[d]) / rng, 2.0 ** -64)
         f[:, 2 * d] = (c - a) / rng * 2.0 - 1.0
-        f[:, 2 * d + 1] = np.log2(w / rng) / 16.0 + 1.0
+        f[:, 2 * d + 1] = np.log2(w) / 16.0 + 1.0
     f[:, 8] = np.asarray(depth, np.float64) / 32.0
     return f.astype(np.float32)
 
