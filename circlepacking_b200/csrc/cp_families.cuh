@@ -38,9 +38,11 @@ __device__ __forceinline__ void trace_put(double* tr, int k, double lhs, double 
 }
 
 // Sub-checks of handle_case_1_1 / handle_case_2_1 (middle_configuration.cu:86-154)
-// given the three collision angles; k0 = bit of the first sub-check.
+// given the three collision angles; k0 = bit of the first sub-check.  The
+// handles are not inlined: one copy each keeps the kernels within the
+// instruction caches (measured 6-9% faster on middle and end_3d).
 template <int MODE>
-__device__ __forceinline__ bool middle_handle(Iv la, Iv r1, Iv r2, Iv r3, bool inner_first, uint8_t& mask, int k0,
+__device__ __noinline__ bool middle_handle(Iv la, Iv r1, Iv r2, Iv r3, bool inner_first, uint8_t& mask, int k0,
                                              bool& trap, double* tr) {
     const double ratio = area_ratio_ub(la);
     const double a1 = disk_area_lb(r1), a2 = disk_area_lb(r2);
@@ -94,7 +96,7 @@ __device__ __forceinline__ bool middle_handle(Iv la, Iv r1, Iv r2, Iv r3, bool i
 
 // handle_inner_outer_2d (INNER) / handle_outer_inner_2d, end_configuration.cu:71-101
 template <bool INNER>
-__device__ __forceinline__ bool end2d_handle(Iv la, Iv r1, Iv r2, bool& trap, double* lhs_out, double* rhs_out) {
+__device__ __noinline__ bool end2d_handle(Iv la, Iv r1, Iv r2, bool& trap, double* lhs_out, double* rhs_out) {
     Iv ca, sa;
     double other_hi, rho_lo;
     if (INNER) {
@@ -124,7 +126,7 @@ __device__ __forceinline__ bool end2d_handle(Iv la, Iv r1, Iv r2, bool& trap, do
 // handle_r1_inner_3d (INNER) / handle_r1_outer_3d, end_configuration.cu:154-210.
 // Returns true when the handle fails; *evaluated = false on the early exit.
 template <bool INNER>
-__device__ __forceinline__ bool end3d_handle(Iv la, Iv r1, Iv r2, Iv r3, bool& trap, bool* evaluated, double* lhs_out,
+__device__ __noinline__ bool end3d_handle(Iv la, Iv r1, Iv r2, Iv r3, bool& trap, bool* evaluated, double* lhs_out,
                                              double* rhs_out) {
     // early exit: definitely(a12 + a23 >= a13)  <=>  a13.hi <= (a12 + a23).lo
     double a12_lo, a23_lo, a13_hi;
