@@ -4,8 +4,12 @@ One step = the box refinement of all six families from a uniform lattice seed
 (64 subdivisions per axis over lambda in [0.5, 0.99], the reference's dependent
 radius ranges), not-proved boxes bisected on every axis (16 children for the
 3-disk families, 8 for the 2-disk ones) down to a bounded depth.  `value` is the
-box throughput of the best form (FP32 enclosure pre-pass + FP64); the plain
-FP64 form runs on the same boxes and both must give identical verdict counts.
+box throughput of the best form, picked per family outside the timed region
+(graph engine or host-driven level loop, kernel shape, FP64 or FP32 pre-pass,
+learned criterion order when faster); the plain FP64 form runs on the same
+boxes and both must give identical verdict counts.  The line also carries the
+full-domain proofs of the families lambda-only refinement closes, one of them
+also proved by the reference's own lambda loop for comparison.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--depth L]
     python bench.py --impl reference     # the CPU restatement on the host cores

@@ -818,11 +818,10 @@ size_t train_smem() { return sizeof(TrainSmem); }
 
 cp_status launch_train(const FamilyModel& f, const bf16* feats, const uint8_t* crit, const int8_t* axis, size_t n,
                        size_t row0, size_t rows, int fam, cudaStream_t st, bool with_step) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_train_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem());
-        attr = true;
-    }
+    // per-device function attribute: set on every call (cheap), so a handle on
+    // another device gets it too
+    cudaError_t e = cudaFuncSetAttribute(k_train_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem());
+    if (e != cudaSuccess) return cp_record_cuda_error(e, CP_ERR_CUDA);
     TrainArgs a;
     a.feats = feats;
     a.crit = crit;
