@@ -239,6 +239,9 @@ def _declare_handle(L):
     L.cp_autotune.argtypes = [P, ctypes.POINTER(RefineOpts), ctypes.POINTER(ctypes.c_int), P]
     L.cp_refine_boxes_static.argtypes = [I, I, I, I, P, P, P, SZ, ctypes.POINTER(RefineReport), P]
     L.cp_set_level_variant.argtypes = [P, I, I, I]
+    L.cp_refine_resume.argtypes = [P, ctypes.POINTER(RefineReport)]
+    L.cp_checkpoint_save.argtypes = [P, ctypes.c_char_p]
+    L.cp_checkpoint_load.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(RefineOpts)]
     L.cp_autotune_graph.argtypes = [P, ctypes.POINTER(RefineOpts), ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_int), P]
 
@@ -366,6 +369,20 @@ class Prover:
             _check(self._L.cp_refine_boxes(self._h, ctypes.byref(o), _ptr(lo), _ptr(hi), _ptr(dp), lo.shape[1],
                                           ctypes.byref(r)), "cp_refine_boxes")
         return r.as_dict()
+
+    def refine_resume(self) -> dict:
+        """Continues the refinement interrupted by interrupt() (or loaded from a checkpoint)."""
+        r = RefineReport()
+        _check(self._L.cp_refine_resume(self._h, ctypes.byref(r)), "cp_refine_resume")
+        return r.as_dict()
+
+    def checkpoint_save(self, path):
+        _check(self._L.cp_checkpoint_save(self._h, os.fsencode(path)), "cp_checkpoint_save")
+
+    def checkpoint_load(self, path) -> RefineOpts:
+        o = RefineOpts()
+        _check(self._L.cp_checkpoint_load(self._h, os.fsencode(path), ctypes.byref(o)), "cp_checkpoint_load")
+        return o
 
     def reference_step(self, family, la_lb, la_ub, sizes=None):
         """One reference-semantics lattice launch: smallest failing lambda.lb (inf if none)."""

@@ -6,6 +6,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <queue>
 #include <vector>
@@ -269,6 +270,10 @@ struct cp_prover {
     unsigned long long graph_key[12] = {0};
     int graph_variant[6][2] = {{1, 1}, {1, 1}, {1, 1}, {1, 1}, {1, 1}, {1, 1}};  // block-size variant
     int graph_bpt[6][2] = {{2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}};      // boxes per thread
+    // an interrupted host-driven refinement: the level stack and counters hold
+    // its remaining boxes and partial counts (cp_refine_resume, checkpoints)
+    bool pending = false;
+    cp_refine_opts pending_opts{};
     int variant[6][2] = {{1, 1}, {0, 0}, {1, 1}, {1, 1}, {0, 0}, {1, 1}};  // level-kernel variant per family/precision
 };
 
@@ -511,6 +516,8 @@ cp_status refine_levels(cp_prover* p, const cp_refine_opts& o, cp_refine_report*
         in.n -= c;
         if (p->interrupt.load()) {
             p->interrupt.store(0);
+            p->pending = true;
+            p->pending_opts = o;
             return CP_ERR_INTERRUPTED;
         }
     }
@@ -752,6 +759,7 @@ void cp_request_interrupt(cp_prover* p) {
 cp_status cp_refine(cp_prover* p, const cp_refine_opts* o, cp_refine_report* r) {
     if (!p || !r) return CP_ERR_INVALID;
     CP_TRY(check_opts(o));
+    p->pending = false;
     const double t0 = now_ms();
     std::memset(r, 0, sizeof(*r));
     CP_TRY(cuda_ok(cudaSetDevice(p->device)));
@@ -840,6 +848,7 @@ cp_status cp_refine_boxes(cp_prover* p, const cp_refine_opts* o, const double* l
                           const uint8_t* depth, size_t n, cp_refine_report* r) {
     if (!p || !r || (n && (!lo || !hi))) return CP_ERR_INVALID;
     CP_TRY(check_opts(o));
+    p->pending = false;
     const double t0 = now_ms();
     std::memset(r, 0, sizeof(*r));
     CP_TRY(cuda_ok(cudaSetDevice(p->device)));
@@ -863,6 +872,7 @@ cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* o, const doub
                                const uint8_t* depth, size_t n, cp_refine_report* r) {
     if (!p || !r || (n && (!lo || !hi))) return CP_ERR_INVALID;
     CP_TRY(check_opts(o));
+    p->pending = false;
     const double t0 = now_ms();
     std::memset(r, 0, sizeof(*r));
     CP_TRY(cuda_ok(cudaSetDevice(p->device)));
@@ -887,9 +897,141 @@ cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* o, const doub
     return run_refinement(p, *o, r, t0);
 }
 
+// ------------------------------------------------------------------ resume / checkpoints
+cp_status cp_refine_resume(cp_prover* p, cp_refine_report* r) {
+    if (!p || !r) return CP_ERR_INVALID;
+    if (!p->pending) return cp_fail(CP_ERR_INVALID, "cp_refine_resume: no interrupted refinement in this handle");
+    const double t0 = now_ms();
+    std::memset(r, 0, sizeof(*r));
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    const cp_refine_opts o = p->pending_opts;
+    p->pending = false;
+    return refine_levels(p, o, r, t0);
+}
+
+}  // extern "C"
+
+namespace {
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, dims;
+    uint32_t opts_size, counter_words;
+    uint64_t level_cap;
+    uint32_t nlevels, reserved;
+    cp_refine_opts opts;
+};
+constexpr char kCkptMagic[8] = {'C', 'P', 'B', '2', 'C', 'K', 'P', 'T'};
+constexpr uint32_t kCkptVersion = 1;
+constexpr size_t kCkptStage = (size_t)1 << 22;  // doubles per staging copy
+
+// Copies `count` elements of device array `dev` to `f` through a host buffer.
+template <class T>
+cp_status dump(std::FILE* f, const T* dev, size_t count, std::vector<unsigned char>& stage, cudaStream_t st) {
+    const size_t per = stage.size() / sizeof(T);
+    for (size_t off = 0; off < count; off += per) {
+        const size_t k = std::min(per, count - off);
+        CP_TRY(cuda_ok(cudaMemcpyAsync(stage.data(), dev + off, k * sizeof(T), cudaMemcpyDeviceToHost, st)));
+        CP_TRY(cuda_ok(cudaStreamSynchronize(st)));
+        if (std::fwrite(stage.data(), sizeof(T), k, f) != k) return cp_fail(CP_ERR_INVALID, "checkpoint: write failed");
+    }
+    return CP_OK;
+}
+template <class T>
+cp_status load(std::FILE* f, T* dev, size_t count, std::vector<unsigned char>& stage, cudaStream_t st) {
+    const size_t per = stage.size() / sizeof(T);
+    for (size_t off = 0; off < count; off += per) {
+        const size_t k = std::min(per, count - off);
+        if (std::fread(stage.data(), sizeof(T), k, f) != k) return cp_fail(CP_ERR_INVALID, "checkpoint: file truncated");
+        CP_TRY(cuda_ok(cudaMemcpyAsync(dev + off, stage.data(), k * sizeof(T), cudaMemcpyHostToDevice, st)));
+        CP_TRY(cuda_ok(cudaStreamSynchronize(st)));
+    }
+    return CP_OK;
+}
+struct FileCloser {
+    std::FILE* f;
+    ~FileCloser() {
+        if (f) std::fclose(f);
+    }
+};
+}  // namespace
+
+extern "C" {
+
+cp_status cp_checkpoint_save(cp_prover* p, const char* path) {
+    if (!p || !path) return CP_ERR_INVALID;
+    if (!p->pending) return cp_fail(CP_ERR_INVALID, "cp_checkpoint_save: no interrupted refinement in this handle");
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    FileCloser fc{std::fopen(path, "wb")};
+    if (!fc.f) return cp_fail(CP_ERR_INVALID, "cp_checkpoint_save: cannot open %s", path);
+    CkptHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, kCkptMagic, 8);
+    h.version = kCkptVersion;
+    h.dims = (uint32_t)family_dims(p->pending_opts.family);
+    h.opts_size = (uint32_t)sizeof(cp_refine_opts);
+    h.counter_words = (uint32_t)(C_COUNT + kDepthBins);
+    h.level_cap = p->level_cap;
+    h.nlevels = (uint32_t)p->levels.size();
+    h.opts = p->pending_opts;
+    if (std::fwrite(&h, sizeof(h), 1, fc.f) != 1) return cp_fail(CP_ERR_INVALID, "checkpoint: write failed");
+    std::vector<uint64_t> n(h.nlevels);
+    for (uint32_t l = 0; l < h.nlevels; ++l) n[l] = p->levels[l].n;
+    if (std::fwrite(n.data(), sizeof(uint64_t), n.size(), fc.f) != n.size())
+        return cp_fail(CP_ERR_INVALID, "checkpoint: write failed");
+    std::vector<unsigned char> stage(sizeof(double) * kCkptStage);
+    CP_TRY(dump(fc.f, p->cnt, h.counter_words, stage, p->stream));
+    for (uint32_t l = 0; l < h.nlevels; ++l) {
+        if (!n[l]) continue;
+        const BoxList& b = p->levels[l].b;
+        for (uint32_t d = 0; d < h.dims; ++d) CP_TRY(dump(fc.f, b.lo + d * b.cap, n[l], stage, p->stream));
+        for (uint32_t d = 0; d < h.dims; ++d) CP_TRY(dump(fc.f, b.hi + d * b.cap, n[l], stage, p->stream));
+        CP_TRY(dump(fc.f, b.depth, n[l], stage, p->stream));
+    }
+    if (std::fflush(fc.f) != 0) return cp_fail(CP_ERR_INVALID, "checkpoint: write failed");
+    return CP_OK;
+}
+
+cp_status cp_checkpoint_load(cp_prover* p, const char* path, cp_refine_opts* opts) {
+    if (!p || !path) return CP_ERR_INVALID;
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    FileCloser fc{std::fopen(path, "rb")};
+    if (!fc.f) return cp_fail(CP_ERR_INVALID, "cp_checkpoint_load: cannot open %s", path);
+    CkptHeader h;
+    if (std::fread(&h, sizeof(h), 1, fc.f) != 1 || std::memcmp(h.magic, kCkptMagic, 8) != 0 ||
+        h.version != kCkptVersion || h.opts_size != sizeof(cp_refine_opts) ||
+        h.counter_words != (uint32_t)(C_COUNT + kDepthBins))
+        return cp_fail(CP_ERR_INVALID, "cp_checkpoint_load: %s is not a checkpoint of this library version", path);
+    CP_TRY(check_opts(&h.opts));
+    if (h.dims != (uint32_t)family_dims(h.opts.family) || h.nlevels == 0 || h.nlevels > 251 || h.level_cap == 0)
+        return cp_fail(CP_ERR_INVALID, "cp_checkpoint_load: inconsistent header in %s", path);
+    std::vector<uint64_t> n(h.nlevels);
+    if (std::fread(n.data(), sizeof(uint64_t), n.size(), fc.f) != n.size())
+        return cp_fail(CP_ERR_INVALID, "checkpoint: file truncated");
+    for (uint64_t k : n)
+        if (k > h.level_cap) return cp_fail(CP_ERR_INVALID, "cp_checkpoint_load: level larger than its capacity");
+    p->pending = false;
+    CP_TRY(ensure_levels(p, (int)h.nlevels, (int)h.dims, (size_t)h.level_cap));
+    std::vector<unsigned char> stage(sizeof(double) * kCkptStage);
+    CP_TRY(load(fc.f, p->cnt, h.counter_words, stage, p->stream));
+    for (auto& L : p->levels) L.n = 0;
+    for (uint32_t l = 0; l < h.nlevels; ++l) {
+        if (!n[l]) continue;
+        BoxList& b = p->levels[l].b;
+        for (uint32_t d = 0; d < h.dims; ++d) CP_TRY(load(fc.f, b.lo + d * b.cap, n[l], stage, p->stream));
+        for (uint32_t d = 0; d < h.dims; ++d) CP_TRY(load(fc.f, b.hi + d * b.cap, n[l], stage, p->stream));
+        CP_TRY(load(fc.f, b.depth, n[l], stage, p->stream));
+        p->levels[l].n = (size_t)n[l];
+    }
+    p->pending = true;
+    p->pending_opts = h.opts;
+    if (opts) *opts = h.opts;
+    return CP_OK;
+}
+
 cp_status cp_reference_step(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,
                             double* first_critical, double* err_box) {
     if (!p || family < 0 || family > 5 || !first_critical) return CP_ERR_INVALID;
+    p->pending = false;  // the counters are reused
     CP_TRY(cuda_ok(cudaSetDevice(p->device)));
     const int D = family_dims(family);
     LatticeSpec s{family, {1, 1, 1, 1}, la_lb, la_ub};
@@ -948,6 +1090,7 @@ cp_status cp_reference_step(cp_prover* p, int family, double la_lb, double la_ub
 cp_status cp_prove_family_reference(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,
                                     int64_t max_launches, double* trace, cp_reference_report* r) {
     if (!p || !r || family < 0 || family > 5) return CP_ERR_INVALID;
+    p->pending = false;  // the counters are reused
     std::memset(r, 0, sizeof(*r));
     const double t0 = now_ms();
     struct Lb {
@@ -1031,6 +1174,7 @@ cp_status cp_prove_family_reference(cp_prover* p, int family, double la_lb, doub
 cp_status cp_reference_criticals(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,
                                  size_t max_boxes, double* boxes, uint8_t* handles, size_t* count) {
     if (!p || family < 0 || family > 5 || !count || (max_boxes && (!boxes || !handles))) return CP_ERR_INVALID;
+    p->pending = false;  // the counters are reused
     CP_TRY(cuda_ok(cudaSetDevice(p->device)));
     const int D = family_dims(family);
     LatticeSpec s{family, {1, 1, 1, 1}, la_lb, la_ub};

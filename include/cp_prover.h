@@ -280,6 +280,27 @@ cp_status cp_div_check(const double* a, const double* b, size_t n, double* out, 
  * reciprocal (rates holds 8 doubles).  Synchronous. */
 cp_status cp_measure_primitives(int device, double* rates);
 
+/* ---------------------------------------------------------------- resume and checkpoints
+ * The reference keeps its only state, the lambda priority queue, in memory and
+ * offers no resume (run_kernel.cuh:71); these entry points let a long
+ * refinement on a shared machine stop and continue.  A host-driven refinement
+ * (CP_ENGINE_LEVELS) stopped by cp_request_interrupt returns CP_ERR_INTERRUPTED
+ * between chunks and leaves its remaining boxes and partial counts in the
+ * handle.  Any other refinement or reference-step call discards that state. */
+
+/* Continues the interrupted refinement of this handle; the report covers the
+ * whole refinement (counts from before the interruption included). */
+cp_status cp_refine_resume(cp_prover* p, cp_refine_report* report);
+
+/* Writes the interrupted refinement (options, counters, the boxes left on every
+ * level) to a binary file. */
+cp_status cp_checkpoint_save(cp_prover* p, const char* path);
+
+/* Reads a checkpoint into this handle (any handle, e.g. in a new process);
+ * cp_refine_resume then continues it.  opts: NULL or receives the options of
+ * the checkpointed refinement. */
+cp_status cp_checkpoint_load(cp_prover* p, const char* path, cp_refine_opts* opts);
+
 /* ---------------------------------------------------------------- autotuning
  * The level kernel is compiled in CP_LEVEL_VARIANTS register/occupancy variants
  * (minimum resident 128-thread blocks per SM 1, 4, 5, 6).  cp_autotune runs
