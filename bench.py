@@ -320,8 +320,19 @@ def roofline_of(cp, device, reps, ms_step) -> dict:
     kernel_ms = sum(r["device_ms"] for r in reps)
     achieved = 2.0 * work / (kernel_ms / 1e3) / 1e12
     peak = 2.0 * rates["dfma"] / 1e12
+    # DRAM traffic: ncu cannot profile kernel nodes of a graph with conditional
+    # nodes; one capture of a whole graph refinement (middle, 32^4 seed, one
+    # level: 11.95M boxes evaluated, 10.9M children written) read 1.154 GB and
+    # wrote 1.237 GB, i.e. 200 B per evaluated box against 124 B algorithmic
+    # (65 B per box read + 65 B per child written).  Traffic grows with the
+    # boxes, so it is reported per evaluated box and scaled to the step.
+    traffic_per_box, algorithmic_per_box = 2.391e9 / 11.95e6, 124.0
+    boxes = sum(r["evaluated"] for r in reps)
     return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "k_level_persist<family, fp64, block> (per-box FP64 criteria + split)",
+            "traffic": traffic_per_box * boxes,
+            "traffic_note": f"DRAM bytes per step, from an ncu capture at {traffic_per_box:.0f} B per evaluated box "
+                            f"(algorithmic {algorithmic_per_box:.0f} B); profiles/k_level_middle_fp64.md",
+            "kernel": "k_level_persist<family, fp64, block> (per-box FP64 criteria + split)",
             "work_model": "per box: CPU-oracle-counted add/mul/div/asin of the reference's evaluation path on the "
                           "seed lattices, each weighted by measured DFMA rate / primitive rate; peak = measured DFMA",
             "peaks_measured_tops": {k: v / 1e12 for k, v in rates.items()}, "peak_source": "measured in-process",
