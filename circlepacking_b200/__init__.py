@@ -445,6 +445,7 @@ def _declare_model(L):
     L.cp_model_set_params.argtypes = [P, I, P]
     L.cp_model_loss_grad.argtypes = [I, P, P, P, P, SZ, P, P]
     L.cp_model_predict.argtypes = [P, I, P, P, P, SZ, P, P, P]
+    L.cp_model_set_inference.argtypes = [P, I]
 
 
 def model_param_count() -> int:
@@ -506,6 +507,11 @@ class _ModelMixin:
         p = np.ascontiguousarray(params, np.float32)
         _check(self._L.cp_model_set_params(self._h, family, p.ctypes.data), "cp_model_set_params")
 
+    def model_set_inference(self, kind):
+        """0: warp-level mma.sync inference kernel; 1: tcgen05 + tensor memory."""
+        _declare_model(self._L)
+        _check(self._L.cp_model_set_inference(self._h, kind), "cp_model_set_inference")
+
     def model_predict(self, family, lo, hi, depth=None):
         _declare_model(self._L)
         lo = np.ascontiguousarray(lo, np.float64)
@@ -520,7 +526,8 @@ class _ModelMixin:
         return logits, axis, order
 
 
-for _name in ("model_collect", "model_records", "model_train", "model_params", "model_set_params", "model_predict"):
+for _name in ("model_collect", "model_records", "model_train", "model_params", "model_set_params", "model_predict",
+              "model_set_inference"):
     setattr(Prover, _name, getattr(_ModelMixin, _name))
 
 

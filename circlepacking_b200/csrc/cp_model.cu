@@ -620,6 +620,225 @@ __global__ void __launch_bounds__(128) k_infer(InferArgs a) {
     }
 }
 
+
+// ------------------------------------------------------------------ inference on tcgen05
+// The same forward pass on the 5th-generation tensor cores: a CTA takes 128
+// boxes (one per thread), stages their features and the weights in shared
+// memory in the canonical K-major core-matrix layout (8 rows x 16 bytes per
+// core matrix; LBO = 128 B between core matrices along K, SBO = K * 16 B
+// between 8-row groups), and one thread issues tcgen05.mma (M = 128, N = 64 or
+// 16, K = 16 per instruction, BF16 in, FP32 accumulators in tensor memory).
+// Every thread reads its box's row back with tcgen05.ld, applies bias and
+// GELU, and writes the next layer's operand tile.  Waits on the MMA-completion
+// mbarrier are bounded: on time-out the kernel raises *err, waits (bounded)
+// once more, frees its tensor memory and returns.
+constexpr int kTcRows = 128;
+constexpr uint32_t kTcCols = 128;  // tensor-memory columns per CTA: [0, 64) hidden, [64, 80) logits
+
+struct TcSmem {
+    bf16 a[kTcRows * NH];  // activation tile (K <= 64)
+    bf16 w1[NH * NK];      // W1^T: N = 64 rows, K = 16
+    bf16 w2[NH * NH];      // W2^T: 64 x 64
+    bf16 w3[16 * NH];      // W3^T padded to N = 16 rows, K = 64
+    float b1[NH], b2[NH], b3[16];
+    unsigned long long mbar;
+    uint32_t tmem;
+};
+
+// element offset of (row, k) in a K-major core-matrix tile with K columns
+__device__ __forceinline__ int cm_off(int row, int k, int K) {
+    return (row >> 3) * (K * 8) + (k >> 3) * 64 + (row & 7) * 8 + (k & 7);
+}
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// shared-memory matrix descriptor (no swizzle, K-major), Blackwell version 1
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128
+__host__ __device__ constexpr uint32_t tc_idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+}
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_ld64(uint32_t taddr, uint32_t* r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t* r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct TcArgs {
+    InferArgs a;
+    int* err;  // raised when an MMA-completion wait times out
+};
+
+template <int FAM>
+__global__ void __launch_bounds__(kTcRows) k_infer_tc(TcArgs ta) {
+    constexpr int D = family_dims(FAM);
+    __shared__ __align__(1024) TcSmem s;
+    const InferArgs& a = ta.a;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    // weights and biases, staged once per CTA
+    for (int i = tid; i < NH * NK; i += kTcRows) s.w1[cm_off(i / NK, i % NK, NK)] = a.views[V_W1T + i];
+    for (int i = tid; i < NH * NH; i += kTcRows) s.w2[cm_off(i / NH, i % NH, NH)] = a.views[V_W2T + i];
+    for (int i = tid; i < 16 * NH; i += kTcRows) {
+        const int n = i / NH, k = i % NH;
+        s.w3[cm_off(n, k, NH)] = n < NO ? a.views[V_W3T + n * NH + k] : __float2bfloat16(0.f);
+    }
+    for (int i = tid; i < NH; i += kTcRows) {
+        s.b1[i] = a.master[P_B1 + i];
+        s.b2[i] = a.master[P_B2 + i];
+    }
+    if (tid < 16) s.b3[tid] = tid < NO ? a.master[P_B3 + tid] : 0.f;
+    const uint32_t mbar = smem_u32(&s.mbar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem)),
+                     "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s.tmem;
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;  // this warp's quadrant of tensor-memory lanes
+    const uint32_t a_addr = smem_u32(s.a), w1_addr = smem_u32(s.w1), w2_addr = smem_u32(s.w2),
+                   w3_addr = smem_u32(s.w3);
+    uint32_t phase = 0;
+    bool ok = true;
+    const size_t tiles = (a.count + kTcRows - 1) / kTcRows;
+    for (size_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const size_t j = tile * kTcRows + tid;
+        // ---- features of this thread's box -> layer-1 operand tile (K = 16)
+        {
+            float f[16];
+            if (j < a.count) {
+                const size_t i = a.begin + j;
+                double lo[4], hi[4];
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    lo[d] = a.in.lo[d * a.in.cap + i];
+                    hi[d] = a.in.hi[d * a.in.cap + i];
+                }
+                const int depth = a.in.depth[i];
+                box_features_fast<D>(lo, hi, depth == 0xFF ? 0 : depth, f);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 16; ++k) f[k] = 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < 16; ++k) s.a[cm_off(tid, k, NK)] = __float2bfloat16_rn(f[k]);
+        }
+        uint32_t r[64];
+#pragma unroll
+        for (int layer = 0; layer < 3; ++layer) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            if (tid == 0) {
+                if (layer == 0) {
+                    tc_mma(tmem, sdesc(a_addr, 128, NK * 16), sdesc(w1_addr, 128, NK * 16), tc_idesc(NH), 0);
+                } else {
+                    const uint32_t w_addr = layer == 1 ? w2_addr : w3_addr;
+                    const uint32_t d_col = layer == 1 ? 0u : 64u;
+                    const uint32_t idesc = tc_idesc(layer == 1 ? NH : 16);
+#pragma unroll
+                    for (int ks = 0; ks < NH / 16; ++ks)
+                        tc_mma(tmem + d_col, sdesc(a_addr + 256 * ks, 128, NH * 16), sdesc(w_addr + 256 * ks, 128, NH * 16),
+                               idesc, ks > 0 ? 1u : 0u);
+                }
+                tc_commit(mbar);
+            }
+            ok = __syncthreads_and(mbar_wait(mbar, phase) ? 1 : 0) != 0;  // block-uniform
+            phase ^= 1u;
+            tc_fence_after();
+            if (!ok) break;
+            if (layer < 2) {
+                tc_ld64(tmem + lane_base, r);
+                const float* bias = layer == 0 ? s.b1 : s.b2;
+                tc_fence_before();
+                __syncthreads();  // every thread has read its row; the tile may be overwritten
+#pragma unroll
+                for (int c = 0; c < NH; ++c)
+                    s.a[cm_off(tid, c, NH)] = __float2bfloat16_rn(gelu_fast(__uint_as_float(r[c]) + bias[c]));
+            } else {
+                tc_ld16(tmem + lane_base + 64u, r);
+            }
+        }
+        if (!ok) break;
+        if (j < a.count) {
+            float z[NO];
+#pragma unroll
+            for (int k = 0; k < NO; ++k) z[k] = __uint_as_float(r[k]) + s.b3[k];
+            int ord = 0;
+            if (FAM == F_MIDDLE)
+                ord = fmaxf(z[2], z[3]) > fmaxf(z[0], z[1]) ? 1 : 0;
+            else if (FAM == F_END_2D || FAM == F_END_3D)
+                ord = z[1] > z[0] ? 1 : 0;
+            int ax = 0;
+            float best = z[4];
+#pragma unroll
+            for (int d = 1; d < D; ++d)
+                if (z[4 + d] > best) {
+                    best = z[4 + d];
+                    ax = d;
+                }
+            if (a.order) a.order[j] = (uint8_t)ord;
+            if (a.axis) a.axis[j] = (uint8_t)ax;
+            if (a.logits)
+                for (int k = 0; k < NO; ++k) a.logits[j * NO + k] = z[k];
+        }
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(ta.err, 1);
+        mbar_wait(mbar, phase);  // bounded: let an MMA still in flight finish before freeing its memory
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
+}
+
 // ------------------------------------------------------------------ trace records
 struct LabelArgs {
     BoxList in;
@@ -741,6 +960,10 @@ struct ModelState {
     double* rec_box = nullptr;
     uint8_t* rec_depth = nullptr;
     unsigned long long* rec_count = nullptr;
+    // inference kernel: 0 = warp-level mma.sync, 1 = tcgen05 with tensor memory
+    int infer_kind = 0;
+    int* tc_err = nullptr;    // device flag raised by a timed-out tcgen05 wait
+    int* tc_err_h = nullptr;  // pinned copy, refreshed after every tcgen05 launch
     // per-chunk hints
     uint8_t* hint_axis = nullptr;
     uint8_t* hint_order = nullptr;
@@ -876,6 +1099,24 @@ cp_status launch_infer(int fam, const InferArgs& a, cudaStream_t st) {
 }
 
 template <int FAM>
+cp_status launch_infer_tc_t(const TcArgs& a, cudaStream_t st) {
+    const size_t tiles = (a.a.count + kTcRows - 1) / kTcRows;
+    const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(tiles, 148 * 4));
+    k_infer_tc<FAM><<<grid, kTcRows, 0, st>>>(a);
+    return cp_check_launch();
+}
+cp_status launch_infer_tc(int fam, const TcArgs& a, cudaStream_t st) {
+    switch (fam) {
+    case 0: return launch_infer_tc_t<0>(a, st);
+    case 1: return launch_infer_tc_t<1>(a, st);
+    case 2: return launch_infer_tc_t<2>(a, st);
+    case 3: return launch_infer_tc_t<3>(a, st);
+    case 4: return launch_infer_tc_t<4>(a, st);
+    default: return launch_infer_tc_t<5>(a, st);
+    }
+}
+
+template <int FAM>
 cp_status launch_label_t(const LabelArgs& a, cudaStream_t st) {
     k_label<FAM><<<148 * 4, 128, 0, st>>>(a);
     return cp_check_launch();
@@ -892,6 +1133,25 @@ cp_status launch_label(int fam, const LabelArgs& a, cudaStream_t st) {
 }
 
 }  // namespace
+
+// Runs the configured inference kernel; with tcgen05, the device error flag of
+// the previous launch is checked first and this launch's flag is copied to
+// pinned memory behind it (the engine synchronises the stream between chunks).
+cp_status run_infer(ModelState* m, int fam, const InferArgs& a, cudaStream_t st) {
+    if (m->infer_kind == 0 || a.sched) return launch_infer(fam, a, st);
+    if (!m->tc_err) {
+        M_TRY(ok_or(cudaMalloc(&m->tc_err, sizeof(int))));
+        M_TRY(ok_or(cudaMallocHost(&m->tc_err_h, sizeof(int))));
+        *m->tc_err_h = 0;
+        M_TRY(ok_or(cudaMemsetAsync(m->tc_err, 0, sizeof(int), st)));
+    }
+    if (*m->tc_err_h) return cp_fail(CP_ERR_DEVICE, "tcgen05 inference: a tensor-core completion wait timed out");
+    TcArgs t;
+    t.a = a;
+    t.err = m->tc_err;
+    M_TRY(launch_infer_tc(fam, t, st));
+    return ok_or(cudaMemcpyAsync(m->tc_err_h, m->tc_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+}
 
 // ------------------------------------------------------------------ engine hooks
 cp_status cp_model_hints(cp_prover* p, int fam, const BoxList& in, size_t begin, size_t count, uint8_t** axis,
@@ -919,7 +1179,7 @@ cp_status cp_model_hints(cp_prover* p, int fam, const BoxList& in, size_t begin,
     a.axis = axis ? m->hint_axis : nullptr;
     a.order = order ? m->hint_order : nullptr;
     a.logits = nullptr;
-    M_TRY(launch_infer(fam, a, cp_prover_stream(p)));
+    M_TRY(run_infer(m, fam, a, cp_prover_stream(p)));
     if (axis) *axis = m->hint_axis;
     if (order) *order = m->hint_order;
     return CP_OK;
@@ -1006,6 +1266,8 @@ void cp_model_free(cp_prover* p) {
     for (auto& f : m->fam) free_family(f);
     free_records(m);
     cudaFree(m->hint_axis);
+    cudaFree(m->tc_err);
+    cudaFreeHost(m->tc_err_h);
     delete m;
     cp_prover_model(p) = nullptr;
 }
@@ -1231,16 +1493,24 @@ cp_status cp_model_predict(cp_prover* p, int family, const double* lo, const dou
             a.axis = dax;
             a.order = dor;
             a.logits = dlg;
-            s = launch_infer(family, a, st);
+            s = run_infer(m, family, a, st);
         }
         if (s == CP_OK && logits)
             s = ok_or(cudaMemcpyAsync(logits, dlg, sizeof(float) * NO * n, cudaMemcpyDeviceToHost, st));
         if (s == CP_OK && axis) s = ok_or(cudaMemcpyAsync(axis, dax, n, cudaMemcpyDeviceToHost, st));
         if (s == CP_OK && order) s = ok_or(cudaMemcpyAsync(order, dor, n, cudaMemcpyDeviceToHost, st));
         if (s == CP_OK) s = ok_or(cudaStreamSynchronize(st));
+        if (s == CP_OK && m->infer_kind && m->tc_err_h && *m->tc_err_h)
+            s = cp_fail(CP_ERR_DEVICE, "tcgen05 inference: a tensor-core completion wait timed out");
     }
     cudaFree(dlo);
     return s;
+}
+
+cp_status cp_model_set_inference(cp_prover* p, int kind) {
+    if (!p || kind < 0 || kind > 1) return cp_fail(CP_ERR_INVALID, "cp_model_set_inference: kind 0 or 1");
+    state(p, true)->infer_kind = kind;
+    return CP_OK;
 }
 
 }  // extern "C"

@@ -360,6 +360,12 @@ cp_status cp_model_set_params(cp_prover* p, int family, const float* params);
 cp_status cp_model_loss_grad(int family, const float* params, const float* feats, const uint8_t* crit,
                              const int8_t* axis, size_t n, float* loss, float* grad);
 
+/* The kernel that runs the network for hints and predictions: 0 = warp-level
+ * BF16 mma.sync (default; also the one used inside the graph engine),
+ * 1 = tcgen05.mma with FP32 accumulators in tensor memory, 128 boxes per CTA
+ * (bounded completion waits; a time-out returns CP_ERR_DEVICE). */
+cp_status cp_model_set_inference(cp_prover* p, int kind);
+
 /* Network outputs for host boxes (lo/hi SoA, stride n; depth may be NULL):
  * logits [n][8], the chosen split axis and criterion order per box. */
 cp_status cp_model_predict(cp_prover* p, int family, const double* lo, const double* hi, const uint8_t* depth,

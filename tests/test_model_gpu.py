@@ -112,3 +112,33 @@ def test_training_gains_over_plain_order(cp, prover):
     assert split["evaluated"] == sum(split["per_depth"])
     print(f"learned split: evaluated {split['evaluated']}, unresolved {split['unresolved']}; "
           f"widest: evaluated {plain['evaluated']}, unresolved {plain['unresolved']}")
+
+
+@pytest.mark.parametrize("family", [3, 5, 1])
+def test_tcgen05_inference_matches_mma_sync(cp, oracle, prover, family):
+    """The tcgen05 (tensor-memory) inference kernel gives the warp-level mma.sync
+    kernel's logits (same BF16 operands; FP32 sums in another order) and the
+    same decisions away from ties."""
+    params = mlp.init_params(31 + family)
+    prover.model_set_params(family, params)
+    dims = boxgen.DIMS[family]
+    idx = boxgen.lattice_indices(family, [64, 16, 16, 8][:dims], 5000, 17)
+    lo, hi = oracle.lattice_boxes(family, boxgen.LAMBDA, [64, 16, 16, 8][:dims], idx)
+    lo, hi = boxgen.sub_boxes(lo, hi, 18)
+    depth = np.random.default_rng(19).integers(0, 30, lo.shape[1]).astype(np.uint8)
+    try:
+        prover.model_set_inference(0)
+        l0, a0, o0 = prover.model_predict(family, lo, hi, depth)
+        prover.model_set_inference(1)
+        l1, a1, o1 = prover.model_predict(family, lo, hi, depth)
+        l1b, _, _ = prover.model_predict(family, lo, hi, depth)  # second call on the same handle
+    finally:
+        prover.model_set_inference(0)
+    assert np.abs(l1 - l0).max() < 1e-3
+    assert (l1b == l1).all()
+    srt = np.sort(l0[:, 4:4 + dims], axis=1)
+    clear = (srt[:, -1] - srt[:, -2]) > 1e-3
+    assert (a1 == a0)[clear].all()
+    want = np.abs(np.maximum(l0[:, 2], l0[:, 3]) - np.maximum(l0[:, 0], l0[:, 1])) > 1e-3 if family == 3 else \
+        np.abs(l0[:, 1] - l0[:, 0]) > 1e-3
+    assert (o1 == o0)[want].all()
