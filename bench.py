@@ -225,21 +225,23 @@ def train_models(prover, cp, depth):
     return out
 
 
-PROOF_SEED = (64, 32, 32, 8)
+# lambda-only proofs: the radius resolution of the seed each family needs
+PROOF_SEEDS = {1: (64, 32, 32), 2: (64, 64, 64, 16), 3: (64, 32, 32, 8), 4: (64, 128, 128), 5: (64, 32, 32, 8)}
 PROOF_DEPTH = 24
-PROOF_FAMILIES = (1, 3, 5)
+PROOF_FAMILIES = (1, 2, 3, 4, 5)
 
 
 def proof_leg(prover, cp, forms, families, world=1):
     """Full-domain proofs: the family's whole domain (lambda in [0.5, 0.99], the
-    dependent radius ranges) from a 64 x 32 x 32 (x 8) lattice seed, not-proved
-    boxes bisected in lambda only -- the reference's own refinement rule
+    dependent radius ranges) from a lattice seed with 64 lambda slabs and the
+    radius resolution the family needs (PROOF_SEEDS), not-proved boxes bisected
+    in lambda only -- the reference's own refinement rule
     (run_kernel.cuh:110-127) -- down to depth 24.  A family is proved when no box
     is left unresolved.  Both forms evaluate the same tree of boxes, so their
     verdict counts must be identical; the best form runs it as one graph launch."""
     out = []
     for f in families:
-        kw = dict(policy=cp.SPLIT_LAMBDA, max_depth=PROOF_DEPTH, seed_sizes=list(PROOF_SEED[:DIMS[f]]),
+        kw = dict(policy=cp.SPLIT_LAMBDA, max_depth=PROOF_DEPTH, seed_sizes=list(PROOF_SEEDS[f]),
                   seed_lambda=SHARD, level_capacity=1 << 23)
         best_kw = dict(kw, precision=forms[f]["precision"], engine=cp.ENGINE_GRAPH,
                        learned_order=forms[f].get("learned_order", False))

@@ -1,13 +1,13 @@
-"""Full-domain proofs on the GPU: the start+end (2 disks), middle and end (3
-disks) families are proved over their whole domain (lambda in [0.5, 0.99] and
-the dependent radius ranges) by lambda-only bisection -- the reference's own
-refinement rule, applied per box -- from a 64 x 32 x 32 (x 8) lattice seed.  Both
-engines evaluate the same tree of boxes."""
+"""Full-domain proofs on the GPU: five of the six families (all but start) are
+proved over their whole domain (lambda in [0.5, 0.99] and the dependent radius
+ranges) by lambda-only bisection -- the reference's own refinement rule, applied
+per box -- from a lattice seed with 64 lambda slabs and the radius resolution
+each family needs.  Both engines evaluate the same tree of boxes."""
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-SEED = (64, 32, 32, 8)
+SEEDS = {1: (64, 32, 32), 2: (64, 64, 64, 16), 3: (64, 32, 32, 8), 4: (64, 128, 128), 5: (64, 32, 32, 8)}
 
 
 @pytest.fixture(scope="module")
@@ -17,9 +17,9 @@ def prover(cp):
     p.close()
 
 
-@pytest.mark.parametrize("family", [1, 3, 5])
+@pytest.mark.parametrize("family", [1, 2, 3, 4, 5])
 def test_family_proved_over_full_domain(cp, prover, family):
-    kw = dict(policy=cp.SPLIT_LAMBDA, max_depth=24, seed_sizes=list(SEED[:cp.DIMS[family]]),
+    kw = dict(policy=cp.SPLIT_LAMBDA, max_depth=24, seed_sizes=list(SEEDS[family]),
               seed_lambda=(cp.LAMBDA_MIN, cp.LAMBDA_MAX), level_capacity=1 << 23)
     a = prover.refine(family, **kw)
     b = prover.refine(family, engine=cp.ENGINE_GRAPH, **kw)
