@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="default kernel shapes, FP64 (profiling runs)")
     ap.add_argument("--no-learned", action="store_true", help="no proposal networks (reference criterion order)")
     ap.add_argument("--no-proof", action="store_true", help="skip the full-domain proof leg")
-    ap.add_argument("--reference-proof", default="3",
+    ap.add_argument("--reference-proof", default="3,5",
                     help="families (comma list, '' = none) whose full-domain proof also runs by the reference's own "
                          "method: its lambda loop over its lattice sizes, on the plain FP64 kernel")
     return ap.parse_args()
