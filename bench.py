@@ -7,9 +7,16 @@ radius ranges), not-proved boxes bisected on every axis (16 children for the
 box throughput of the best form, picked per family outside the timed region
 (graph engine or host-driven level loop, kernel shape, FP64 or FP32 pre-pass,
 learned criterion order when faster); the plain FP64 form runs on the same
-boxes and both must give identical verdict counts.  The line also carries the
-full-domain proofs of the families lambda-only refinement closes, one of them
-also proved by the reference's own lambda loop for comparison.
+boxes, and both must give the same per-box verdict digest (every evaluated box
+and its verdict, hashed on the device).
+
+Beside the headline the line carries: the uneven-depth worklist (64^4 lattice
+plus 10M seeded random boxes at depths 0-8), the FP32 pre-pass form of the
+whole step, the learned criterion order and learned split on the uneven-depth
+worklist, the full-domain proofs of the families lambda-only refinement closes
+(one or two of them also by the reference's own lambda loop), the roofline of
+the level kernel on the reference kernel's own operation counts, and the CPU
+restatement on the host cores.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--depth L]
     python bench.py --impl reference     # the CPU restatement on the host cores
@@ -38,6 +45,15 @@ LEVEL_CAP = 1 << 25
 SHARD = (0.5, 0.9900000000000001)  # this rank's lambda piece (the whole domain on one GPU)
 
 
+_T0 = time.perf_counter()
+
+
+def log(msg: str):
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    sys.stderr.write(f"[bench {time.perf_counter() - _T0:7.1f}s] {msg}\n")
+    sys.stderr.flush()
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -57,7 +73,11 @@ def parse():
     ap.add_argument("--no-proof", action="store_true", help="skip the full-domain proof leg")
     ap.add_argument("--reference-proof", default="3,5",
                     help="families (comma list, '' = none) whose full-domain proof also runs by the reference's own "
-                         "method: its lambda loop over its lattice sizes, on the plain FP64 kernel")
+                         "method: its lambda loop over its lattice sizes, on this library's FP64 lattice kernel")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-depth worklist legs")
+    ap.add_argument("--uneven-family", type=int, default=3, help="family of the uneven-depth worklist legs")
+    ap.add_argument("--uneven-random", type=int, default=10_000_000, help="random boxes added to the lattice seed")
+    ap.add_argument("--no-fp32-leg", action="store_true", help="skip the FP32 pre-pass form of the whole step")
     return ap.parse_args()
 
 
@@ -159,18 +179,26 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- workload
-def seed_opts(family, form, depth):
+def seed_opts(family, form, depth, digest=False):
     """Refinement options of one family in a form: {"precision", "engine", "learned_order"}."""
     import circlepacking_b200 as cp
 
     return dict(precision=form["precision"], policy=cp.SPLIT_UNIFORM, max_depth=depth,
                 seed_sizes=[SEED_RES] * DIMS[family], seed_lambda=SHARD,
-                level_capacity=LEVEL_CAP, engine=form["engine"], learned_order=form.get("learned_order", False))
+                level_capacity=LEVEL_CAP, engine=form["engine"], learned_order=form.get("learned_order", False),
+                digest=digest)
 
 
-def run_step(prover, forms, depth):
+def run_step(prover, forms, depth, digest=False):
     """One step: the refinement of every family in its form."""
-    return [prover.refine(f, **seed_opts(f, forms[f], depth)) for f in FAMILIES]
+    return [prover.refine(f, **seed_opts(f, forms[f], depth, digest)) for f in FAMILIES]
+
+
+def same_boxes_and_verdicts(a, b):
+    """Two reports of refinements that must have evaluated the same boxes with
+    the same verdicts: equal per-box digests (and counts)."""
+    return (a["digest"] == b["digest"] and a["digest"] != (0, 0) and a["verdicts"] == b["verdicts"]
+            and a["unresolved"] == b["unresolved"] and a["per_depth"] == b["per_depth"])
 
 
 def autotune(prover, cp, learned: bool):
@@ -225,6 +253,13 @@ def train_models(prover, cp, depth):
     return out
 
 
+# DRAM traffic of the graph refinement per evaluated box, from one ncu capture
+# (middle family, 32^4 seed, one level: 11.95M boxes evaluated, 10.9M children
+# written, 1.154 GB read + 1.237 GB written); algorithmic: 65 B read per 4-D box
+# and 65 B written per child.  FP64 pipe activity of the same capture.
+TRAFFIC_PER_BOX, ALGORITHMIC_BYTES_PER_BOX = 2.391e9 / 11.95e6, 124.0
+FP64_PIPE_ACTIVE_NCU = 0.209
+
 # lambda-only proofs: the radius resolution of the seed each family needs
 PROOF_SEEDS = {1: (64, 32, 32), 2: (64, 64, 64, 16), 3: (64, 32, 32, 8), 4: (64, 128, 128), 5: (64, 32, 32, 8)}
 PROOF_DEPTH = 24
@@ -256,7 +291,9 @@ def proof_leg(prover, cp, forms, families, world=1):
         t0 = time.perf_counter()
         p = prover.refine(f, **plain_kw)
         tp = time.perf_counter() - t0
-        same = all(b[k] == p[k] for k in ("evaluated", "verdicts", "unresolved", "clipped", "per_depth"))
+        # verdict identity box by box: one more run of each form with the digest on
+        same = same_boxes_and_verdicts(prover.refine(f, digest=True, **best_kw),
+                                       prover.refine(f, digest=True, **plain_kw))
         # over all ranks' lambda pieces: counts summed, times the slowest rank's
         unresolved = sum_over_ranks(world, b["unresolved"] + p["unresolved"])
         out.append({"family": cp.FAMILIES[f], "proved": unresolved == 0,
@@ -288,58 +325,98 @@ def seed_boxes_host(family):
     return hlo, hhi, hdp
 
 
-def roofline_work():
-    """Primitive-op counts per box (CPU oracle, the reference's evaluation path)
-    on a sample of each family's seed lattice."""
+def sample_evaluated_boxes(prover, cp, depth):
+    """A sample of the boxes the step evaluates, per family and depth: every
+    16th box of every chunk of the same uniform refinement from a 16^dims seed
+    down to `depth` levels, recorded by the device (outside the timed region)."""
+    out = {}
+    rng = np.random.default_rng(5)
+    for f in FAMILIES:
+        prover.model_collect(f, 1_500_000, sample_stride=16, policy=cp.SPLIT_UNIFORM, max_depth=depth,
+                             seed_sizes=[16] * DIMS[f], seed_lambda=SHARD, level_capacity=LEVEL_CAP)
+        r = prover.model_records()
+        d = DIMS[f]
+        boxes, dep = r["boxes"], r["depth"].astype(np.int64)
+        keep = np.zeros(dep.size, bool)
+        for k in np.unique(dep):  # at most 40k boxes per depth
+            idx = np.flatnonzero(dep == k)
+            keep[rng.choice(idx, size=min(idx.size, 40_000), replace=False)] = True
+        out[f] = (boxes[keep, 0:2 * d:2].T.copy(), boxes[keep, 1:2 * d:2].T.copy(), dep[keep])
+    return out
+
+
+def op_counts(samples):
+    """Primitive operations per evaluated box of the reference kernel's own path
+    (stop at the first failing sub-check and handle), per family and depth,
+    counted by the CPU restatement's op-counting mode on the sampled boxes.
+    Runs inside the CPU-baseline leg (the restatement is the checker here)."""
     from oracle import oracle as O
 
-    counts = {}
-    rng = np.random.default_rng(0)
-    for f in FAMILIES:
-        dims = DIMS[f]
-        total = SEED_RES ** dims
-        idx = np.sort(rng.choice(total, size=min(4000, total), replace=False))
-        lo, hi = O.lattice_boxes(f, (0.5, 0.9900000000000001), [SEED_RES] * dims, idx)
-        counts[f] = O.count_ops(f, lo, hi)
-    return counts
+    out = {}
+    for f, (lo, hi, dep) in samples.items():
+        per = {}
+        for d in np.unique(dep):
+            sel = dep == d
+            c = O.count_ops(f, lo[:, sel], hi[:, sel], decide=True)
+            per[int(d)] = {k: c[k] / c["boxes"] for k in ("add", "mul", "div", "asin")} | {"boxes": c["boxes"]}
+        out[f] = per
+    return out
 
 
-def roofline_of(cp, device, reps, ms_step) -> dict:
-    """Roofline of the FP64 criterion evaluation: DFMA-equivalent work per box
-    (each primitive of the reference's evaluation path, counted by the CPU
-    oracle, weighted by the measured DFMA rate over that primitive's measured
-    rate -- the library's own directed division for divisions) against the
-    measured DFMA peak, over the device time of the timed step."""
+def roofline_of(cp, device, reps, counts) -> dict:
+    """Roofline of the FP64 criterion evaluation (the level kernel): the
+    reference kernel's own primitive operations per evaluated box (add/sub,
+    mul, div, asin, each counting one), weighted by the step's boxes per depth,
+    per second of the step's device time, against the measured FP64 instruction
+    peak (one DFMA per lane and cycle).  Two weighted readings stand beside it:
+    each primitive weighted by DFMA rate / its own measured rate, once with the
+    reference's __ddiv_rd and once with this library's division."""
     rates = cp.measure_primitives(device)
-    counts = roofline_work()
-    work = 0.0
+    ops = {"add": 0.0, "mul": 0.0, "div": 0.0, "asin": 0.0}
+    boxes = 0
     for f, r in zip(FAMILIES, reps):
-        c = counts[f]
-        per_box = (c["add"] * rates["dfma"] / rates["dadd_rd"] + c["mul"] * rates["dfma"] / rates["dmul_rd"]
-                   + c["div"] * rates["dfma"] / rates["div_rd_lib"] + c["asin"] * rates["dfma"] / rates["asin"]
-                   ) / c["boxes"]
-        work += r["evaluated"] * per_box
-    kernel_ms = sum(r["device_ms"] for r in reps)
-    achieved = 2.0 * work / (kernel_ms / 1e3) / 1e12
-    peak = 2.0 * rates["dfma"] / 1e12
-    # DRAM traffic: ncu cannot profile kernel nodes of a graph with conditional
-    # nodes; one capture of a whole graph refinement (middle, 32^4 seed, one
-    # level: 11.95M boxes evaluated, 10.9M children written) read 1.154 GB and
-    # wrote 1.237 GB, i.e. 200 B per evaluated box against 124 B algorithmic
-    # (65 B per box read + 65 B per child written).  Traffic grows with the
-    # boxes, so it is reported per evaluated box and scaled to the step.
-    traffic_per_box, algorithmic_per_box = 2.391e9 / 11.95e6, 124.0
-    boxes = sum(r["evaluated"] for r in reps)
-    return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": traffic_per_box * boxes,
-            "traffic_note": f"DRAM bytes per step, from an ncu capture at {traffic_per_box:.0f} B per evaluated box "
-                            f"(algorithmic {algorithmic_per_box:.0f} B); profiles/k_level_middle_fp64.md",
-            "kernel": "k_level_persist<family, fp64, block> (per-box FP64 criteria + split)",
-            "work_model": "per box: CPU-oracle-counted add/mul/div/asin of the reference's evaluation path on the "
-                          "seed lattices, each weighted by measured DFMA rate / primitive rate; peak = measured DFMA",
-            "peaks_measured_tops": {k: v / 1e12 for k, v in rates.items()}, "peak_source": "measured in-process",
-            "ops_per_box": {cp.FAMILIES[f]: {k: counts[f][k] / counts[f]["boxes"] for k in ("add", "mul", "div", "asin")}
-                            for f in FAMILIES}}
+        per = counts[f]
+        depths = sorted(per)
+        for d, n in enumerate(r["per_depth"]):
+            if not n:
+                continue
+            use = per[d] if d in per else per[min(depths, key=lambda x: abs(x - d))]
+            for k in ops:
+                ops[k] += n * use[k]
+            boxes += n
+    kernel_s = sum(r["device_ms"] for r in reps) / 1e3
+    unweighted = sum(ops.values())
+    peak = rates["dfma"]
+
+    def weighted(div_rate):
+        return (ops["add"] * peak / rates["dadd_rd"] + ops["mul"] * peak / rates["dmul_rd"]
+                + ops["div"] * peak / div_rate + ops["asin"] * peak / rates["asin"])
+
+    achieved = unweighted / kernel_s
+    return {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+            "frac": achieved / peak,
+            "traffic": TRAFFIC_PER_BOX * boxes,
+            "traffic_note": f"DRAM bytes per step: {TRAFFIC_PER_BOX:.0f} B per evaluated box from one ncu capture of "
+                            f"the graph refinement (algorithmic {ALGORITHMIC_BYTES_PER_BOX:.0f} B), scaled by the "
+                            f"step's {boxes} evaluated boxes",
+            "kernel": "k_level_persist<family, precision, block> (per-box criteria + split), graph engine",
+            "work_model": "per evaluated box: the reference kernel's own add/sub, mul, div and asin count (it stops "
+                          "at the first failing sub-check and handle), from the CPU restatement's op-counting mode on "
+                          "device-recorded samples of the step's boxes, per depth; each primitive counts 1 against "
+                          "the FP64 instruction peak (DFMA per lane per cycle)",
+            "ops_per_second": {k: v / kernel_s / 1e12 for k, v in ops.items()} | {"unit": "T/s"},
+            "frac_weighted_ddiv_rd": weighted(rates["ddiv_rd"]) / kernel_s / peak,
+            "frac_weighted_library_div": weighted(rates["div_rd_lib"]) / kernel_s / peak,
+            "fp64_pipe_active_ncu": FP64_PIPE_ACTIVE_NCU,
+            "peaks_measured_tops": {k: v / 1e12 for k, v in rates.items()},
+            "peak_source": "measured in-process (MEASURED_PEAKS.json has no FP64 figure): DFMA instruction rate",
+            "ops_per_box": {cp.FAMILIES[f]: {str(d): v for d, v in counts[f].items()} for f in FAMILIES}}
+
+
+def cpu_leg(seconds: float, samples):
+    """The CPU-baseline leg: the CPU restatement timed on the host cores, and its
+    op-counting mode on the sampled boxes of the step (for the roofline)."""
+    return cpu_baseline(seconds), (op_counts(samples) if samples else None)
 
 
 def cpu_baseline(seconds: float) -> dict:
@@ -368,6 +445,108 @@ def cpu_baseline(seconds: float) -> dict:
             "sample": f"{total_boxes} boxes drawn from the 64^dims seed lattices of the families "
                       f"({', '.join(str(f) for f in FAMILIES)}) in {rounds} rounds, CPU restatement "
                       f"(oracle/cpu_oracle.cpp), {threads} threads, {t_total:.1f} s of evaluation"}
+
+
+def uneven_seeds(prover, cp, family, n_random):
+    """The uneven-depth worklist: the family's 64^dims lattice seed (depth 0)
+    followed by n_random seeded random boxes (seed 0xC1C1E5, log-uniform widths
+    2^-20..2^-4, depth labels 0..8), as device tensors."""
+    import torch
+
+    dims = DIMS[family]
+    total = SEED_RES ** dims
+    lo, hi, vis = cp.lattice_boxes(family, SHARD, [SEED_RES] * dims, torch.arange(total, device="cuda"),
+                                   visited=True)
+    rlo, rhi, rdp = prover.random_boxes(family, n_random, seed=0xC1C1E5, max_label=8)
+    dp = torch.where(vis != 0, 0, 255).to(torch.uint8)
+    return (torch.cat([lo, rlo], 1).contiguous(), torch.cat([hi, rhi], 1).contiguous(),
+            torch.cat([dp, rdp]).contiguous())
+
+
+def uneven_legs(prover, cp, forms, args, models_ready):
+    """Uneven-depth worklist of one family, seeded with its 64^dims lattice plus
+    10M random boxes at depths 0..8, refined with the uniform split down to the
+    step's depth: every box is evaluated once; boxes above the depth limit that
+    are not proved get their children evaluated too.  Forms: the best form
+    (graph engine: one persistent kernel over the whole worklist, autotuned
+    shape, the family's precision), the plain FP64 level loop, the best form with
+    the learned criterion order, and the learned split axis (another tree).
+    Each form's verdicts are compared box by box with the plain form's digest."""
+    import torch
+
+    f = args.uneven_family
+    lo, hi, dp = uneven_seeds(prover, cp, f, args.uneven_random)
+    cap = max(LEVEL_CAP, lo.shape[1])
+    base = dict(policy=cp.SPLIT_UNIFORM, max_depth=args.depth, level_capacity=cap)
+    best_kw = dict(base, precision=forms[f]["precision"], engine=cp.ENGINE_GRAPH)
+    plain_kw = dict(base, precision=cp.FP64, engine=cp.ENGINE_LEVELS)
+
+    def timed(kw, reps=2):
+        prover.refine_boxes(f, lo, hi, depth=dp, **kw)  # warm-up (graph build)
+        best = None
+        for _ in range(reps):
+            r = prover.refine_boxes(f, lo, hi, depth=dp, **kw)
+            best = r if best is None or r["device_ms"] < best["device_ms"] else best
+        return best
+
+    def entry(r, ref=None):
+        e = {"evaluated": r["evaluated"], "boxes_per_s": r["evaluated"] / (r["device_ms"] / 1e3),
+             "device_ms": r["device_ms"], "unresolved": r["unresolved"], "per_depth": r["per_depth"],
+             "criteria_per_box": r["handles_evaluated"] / max(1, r["evaluated"]),
+             "fp32_decided_fraction": r["fp32_decided"] / max(1, r["evaluated"])}
+        if ref is not None:
+            e["verdicts_identical"] = same_boxes_and_verdicts(r, ref)
+        return e
+
+    prover.set_level_variant(f, cp.FP64, 0)
+    plain = timed(plain_kw)
+    plain_dig = prover.refine_boxes(f, lo, hi, depth=dp, digest=True, **plain_kw)
+    best = timed(best_kw)
+    best_dig = prover.refine_boxes(f, lo, hi, depth=dp, digest=True, **best_kw)
+    out = {"family": cp.FAMILIES[f], "seeds": int(lo.shape[1]),
+           "seed_depths": np.bincount(dp.cpu().numpy(), minlength=256)[:9].tolist(),
+           "dropped_random_boxes": int((dp == 255).sum().item()),
+           "workload": f"64^dims lattice seed + {args.uneven_random} random boxes (seed 0xC1C1E5, widths 2^-20..2^-4 "
+                       f"log-uniform, depth labels 0..8), uniform split to depth {args.depth}",
+           "plain_fp64": entry(plain), "best": dict(entry(best, plain_dig), form=
+                                                      {"engine": "graph", "precision": "fp64" if
+                                                       forms[f]["precision"] == cp.FP64 else "fp32-prefilter"})}
+    out["best"]["verdicts_identical"] = same_boxes_and_verdicts(best_dig, plain_dig)
+    out["best"]["speedup_vs_plain"] = plain["device_ms"] / best["device_ms"]
+    if models_ready and cp.N_CRITERIA[f] > 1:
+        lrn = timed(dict(best_kw, learned_order=True))
+        lrn_dig = prover.refine_boxes(f, lo, hi, depth=dp, digest=True, learned_order=True, **best_kw)
+        e = entry(lrn)
+        e["verdicts_identical"] = same_boxes_and_verdicts(lrn_dig, plain_dig)
+        e["time_vs_best"] = lrn["device_ms"] / best["device_ms"]
+        e["time_vs_plain"] = lrn["device_ms"] / plain["device_ms"]
+        out["learned_order"] = e
+        split = timed(dict(best_kw, policy=cp.SPLIT_LEARNED), reps=1)
+        e = entry(split)
+        e["note"] = "learned split axis: another tree of boxes (per-box verdicts are the FP64 kernel's own)"
+        out["learned_split"] = e
+    prover.set_level_variant(f, cp.FP64, forms[f].get("variant", 1))
+    del lo, hi, dp
+    torch.cuda.empty_cache()
+    return out
+
+
+def fp32_leg(prover, cp, args, plain_digests):
+    """The FP32 pre-pass form of the whole step (every family, graph engine):
+    time, the fraction of boxes the FP32 pass decides, and per-box verdict
+    identity with the plain FP64 form."""
+    forms = {f: {"precision": cp.FP32_PREFILTER, "engine": cp.ENGINE_GRAPH} for f in FAMILIES}
+    run_step(prover, forms, args.depth)  # warm-up
+    reps = run_step(prover, forms, args.depth)
+    digs = run_step(prover, forms, args.depth, digest=True)
+    boxes = sum(r["evaluated"] for r in reps)
+    ms = sum(r["device_ms"] for r in reps)
+    return {"boxes_per_s": boxes / (ms / 1e3), "device_ms": ms,
+            "fp32_decided_fraction": sum(r["fp32_decided"] for r in reps) / max(1, boxes),
+            "per_family_fp32_decided": {cp.FAMILIES[f]: r["fp32_decided"] / max(1, r["evaluated"])
+                                        for f, r in zip(FAMILIES, reps)},
+            "per_family_device_ms": {cp.FAMILIES[f]: r["device_ms"] for f, r in zip(FAMILIES, reps)},
+            "verdicts_identical": all(same_boxes_and_verdicts(d, p) for d, p in zip(digs, plain_digests))}
 
 
 def main_reference(args, world, rank):
@@ -429,15 +608,18 @@ def main():
         for f in FAMILIES:
             prover.set_level_variant(f, FP64, 0 if on else tuned_variant[f])
 
-    # ---- warm-up (also the verdict-identity check between the two forms)
+    log("autotuned: " + json.dumps({cp.FAMILIES[f]: {k: v for k, v in tuning[cp.FAMILIES[f]].items() if k != "candidates_ms"} for f in FAMILIES}))
+    # ---- warm-up, then the per-box verdict identity of the two forms (one
+    # step each with the device digest of every evaluated box and its verdict)
     for _ in range(max(args.warmup, 3)):
-        best = run_step(prover, forms, args.depth)
+        run_step(prover, forms, args.depth)
+    best_dig = run_step(prover, forms, args.depth, digest=True)
     use_plain(True)
-    plain = run_step(prover, plain_forms, args.depth)
+    plain_dig = run_step(prover, plain_forms, args.depth, digest=True)
     use_plain(False)
-    identical = all(b["verdicts"] == p["verdicts"] and b["unresolved"] == p["unresolved"]
-                    and b["per_depth"] == p["per_depth"] for b, p in zip(best, plain))
+    identical = all(same_boxes_and_verdicts(b, p) for b, p in zip(best_dig, plain_dig))
 
+    log(f"warm-up done; verdicts identical: {identical}")
     # ---- timed: K steps on the prover's stream
     def timed(fm):
         barrier(world)
@@ -469,6 +651,7 @@ def main():
                                          (2 if forms[f].get("learned_order") else 1)) + 2
                         for f, r in zip(FAMILIES, reps_best))
 
+    log(f"timed: best {ms_best:.1f} ms/step, plain {ms_plain:.1f} ms/step")
     # ---- e2e: the host-buffer C-ABI call (seed boxes from pinned host memory)
     e2e = None
     if not args.no_e2e:
@@ -499,6 +682,14 @@ def main():
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3,
                "call": "cp_refine_boxes_host per family (host seed boxes, report back), best form"}
 
+    log("e2e done")
+    # ---- the FP32 pre-pass form of the whole step, and the uneven-depth worklist
+    fp32 = None if args.no_fp32_leg else fp32_leg(prover, cp, args, plain_dig)
+    uneven = None
+    if not args.no_uneven and args.uneven_family in FAMILIES and world == 1:
+        uneven = uneven_legs(prover, cp, forms, args, models_ready=models is not None)
+
+    log("fp32 / uneven legs done")
     # ---- full-domain proofs of the families that lambda-only refinement closes
     proofs = None if args.no_proof else proof_leg(prover, cp, forms, [f for f in PROOF_FAMILIES if f in FAMILIES], world)
     if proofs is not None and args.reference_proof:
@@ -513,16 +704,25 @@ def main():
             t_ref = time.perf_counter() - t0
             for e in proofs:
                 if e["family"] == cp.FAMILIES[f]:
-                    e["reference_method"] = {"proved": ref["proved"], "wall_ms": t_ref * 1e3,
-                                             "device_ms": ref["device_ms"], "launches": ref["launches"],
-                                             "boxes": ref["boxes_evaluated"],
-                                             "lattice": list(cp.REFERENCE_SIZES[f][:DIMS[f]])}
-                    e["speedup_vs_reference_method"] = t_ref * 1e3 / e["best_wall_ms"]
+                    e["reference_method_library_kernel"] = {
+                        "method": "the reference's lambda loop (run_kernel.cuh:61-132) over its lattice sizes, each "
+                                  "launch on this library's slab-ordered FP64 lattice kernel (not the reference's "
+                                  "own kernels)",
+                        "proved": ref["proved"], "wall_ms": t_ref * 1e3, "device_ms": ref["device_ms"],
+                        "launches": ref["launches"], "boxes": ref["boxes_evaluated"],
+                        "lattice": list(cp.REFERENCE_SIZES[f][:DIMS[f]])}
+                    e["speedup_vs_reference_method_library_kernel"] = t_ref * 1e3 / e["best_wall_ms"]
     use_plain(False)
 
-    # ---- roofline of the FP64 criterion kernel (best form)
-    roofline = None if args.no_roofline else roofline_of(cp, local, reps_best, ms_best)
-    cpu = cpu_baseline(args.cpu_seconds) if (rank == 0 and not args.no_cpu) else None
+    log("proofs done")
+    # ---- CPU leg (rank 0): the CPU restatement timed on the host cores, and its
+    # op count of the reference kernel's path on device-recorded samples of the
+    # step's boxes; then the roofline of the level kernel (best form)
+    cpu, counts = None, None
+    if rank == 0 and not args.no_cpu:
+        samples = None if args.no_roofline else sample_evaluated_boxes(prover, cp, args.depth)
+        cpu, counts = cpu_leg(args.cpu_seconds, samples)
+    roofline = roofline_of(cp, local, reps_best, counts) if counts else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_best, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -538,13 +738,18 @@ def main():
         "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain,
                        "form": "fp64, host-driven level loop, kernel variant 0, reference criterion order"},
         "verdicts_identical": identical,
+        "verdicts_identical_by": "device digest (sum and xor of a 64-bit hash of every evaluated box's bounds and "
+                                 "verdict) equal between the best and plain forms, per family",
         "fp32_decided_fraction": sum(r["fp32_decided"] for r in reps_best) / max(1, boxes_step),
+        "fp32_prepass_step": fp32,
+        "uneven_depth_worklist": uneven,
         "criteria_per_box": {"best": sum(r["handles_evaluated"] for r in reps_best) / max(1, boxes_step),
                              "plain": sum(r["handles_evaluated"] for r in reps_plain) /
                              max(1, sum(r["evaluated"] for r in reps_plain))},
         "per_family": [{"family": cp.FAMILIES[f], "evaluated": r["evaluated"], "verdicts": r["verdicts"],
-                        "unresolved": r["unresolved"], "fp32_decided": r["fp32_decided"], "device_ms": r["device_ms"]}
-                       for f, r in zip(FAMILIES, reps_best)],
+                        "unresolved": r["unresolved"], "fp32_decided": r["fp32_decided"], "device_ms": r["device_ms"],
+                        "plain_device_ms": p["device_ms"], "digest": ["%016x" % x for x in d["digest"]]}
+                       for f, r, p, d in zip(FAMILIES, reps_best, reps_plain, best_dig)],
         "full_domain_proofs": proofs,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
         "gpu_launches": launches_step * args.steps,

@@ -193,20 +193,22 @@ class RefineOpts(ctypes.Structure):
     _fields_ = [("family", ctypes.c_int32), ("precision", ctypes.c_int32), ("policy", ctypes.c_int32),
                 ("max_depth", ctypes.c_int32), ("seed_sizes", ctypes.c_int32 * 4), ("seed_lambda", ctypes.c_double * 2),
                 ("level_capacity", ctypes.c_int64), ("block", ctypes.c_int32), ("learned_order", ctypes.c_int32),
-                ("engine", ctypes.c_int32), ("boxes_per_thread", ctypes.c_int32), ("lambda_scale", ctypes.c_double)]
+                ("engine", ctypes.c_int32), ("boxes_per_thread", ctypes.c_int32), ("lambda_scale", ctypes.c_double),
+                ("digest", ctypes.c_int32)]
 
 
 class RefineReport(ctypes.Structure):
     _fields_ = [("evaluated", ctypes.c_int64), ("verdicts", ctypes.c_int64 * 5), ("unresolved", ctypes.c_int64),
                 ("clipped", ctypes.c_int64), ("fp32_decided", ctypes.c_int64), ("per_depth", ctypes.c_int64 * 64),
                 ("max_depth_seen", ctypes.c_int32), ("launches", ctypes.c_int32), ("device_ms", ctypes.c_double),
-                ("wall_ms", ctypes.c_double), ("handles_evaluated", ctypes.c_int64)]
+                ("wall_ms", ctypes.c_double), ("handles_evaluated", ctypes.c_int64), ("digest", ctypes.c_uint64 * 2)]
 
     def as_dict(self) -> dict:
         return dict(evaluated=self.evaluated, verdicts=list(self.verdicts), unresolved=self.unresolved,
                     clipped=self.clipped, fp32_decided=self.fp32_decided,
-                    per_depth=list(self.per_depth)[: self.max_depth_seen + 1], launches=self.launches,
-                    device_ms=self.device_ms, wall_ms=self.wall_ms, handles_evaluated=self.handles_evaluated)
+                    per_depth=list(self.per_depth)[: self.max_depth_seen + 1], max_depth_seen=self.max_depth_seen,
+                    launches=self.launches, device_ms=self.device_ms, wall_ms=self.wall_ms,
+                    handles_evaluated=self.handles_evaluated, digest=(int(self.digest[0]), int(self.digest[1])))
 
 
 class ReferenceReport(ctypes.Structure):
@@ -244,15 +246,16 @@ def _declare_handle(L):
     L.cp_checkpoint_load.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(RefineOpts)]
     L.cp_autotune_graph.argtypes = [P, ctypes.POINTER(RefineOpts), ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_int), P]
+    L.cp_random_boxes.argtypes = [P, I, ctypes.c_uint64, I, SZ, P, P, P]
 
 
 def measure_primitives(device: int = 0) -> dict:
     L = lib()
     _declare_handle(L)
-    rates = np.zeros(8, np.float64)
+    rates = np.zeros(9, np.float64)
     _check(L.cp_measure_primitives(device, rates.ctypes.data), "cp_measure_primitives")
-    return dict(zip(("dfma", "dadd_rd", "dmul_rd", "ddiv_rd", "asin", "ffma", "div_rd_lib", "div_rd_f32seed"),
-                    rates.tolist()))
+    return dict(zip(("dfma", "dadd_rd", "dmul_rd", "ddiv_rd", "asin", "ffma", "div_rd_lib", "div_rd_f32seed_inline",
+                     "div_rd_inline"), rates.tolist()))
 
 
 def div_check(a, b):
@@ -307,7 +310,7 @@ class Prover:
     @staticmethod
     def opts(family, precision=FP64, policy=SPLIT_UNIFORM, max_depth=2, seed_sizes=None, seed_lambda=None,
              level_capacity=0, learned_order=False, engine=ENGINE_LEVELS, block=0, boxes_per_thread=0,
-             lambda_scale=0.0) -> RefineOpts:
+             lambda_scale=0.0, digest=False) -> RefineOpts:
         o = RefineOpts()
         o.family, o.precision, o.policy, o.max_depth = family, precision, policy, max_depth
         ss = list(seed_sizes or [64] * DIMS[family]) + [1] * 4
@@ -321,6 +324,7 @@ class Prover:
         o.engine = engine
         o.boxes_per_thread = boxes_per_thread
         o.lambda_scale = lambda_scale
+        o.digest = int(bool(digest))
         return o
 
     def autotune(self, family, **kw):
@@ -369,6 +373,18 @@ class Prover:
             _check(self._L.cp_refine_boxes(self._h, ctypes.byref(o), _ptr(lo), _ptr(hi), _ptr(dp), lo.shape[1],
                                           ctypes.byref(r)), "cp_refine_boxes")
         return r.as_dict()
+
+    def random_boxes(self, family, n, seed=0xC1C1E5, max_label=8):
+        """n seeded random boxes on the family's domain (cp_random_boxes):
+        CUDA tensors lo, hi of shape (dims, n) and depth labels uint8[n] (255 = dropped)."""
+        torch = _torch()
+        lo = torch.empty((DIMS[family], n), dtype=torch.float64, device="cuda")
+        hi = torch.empty_like(lo)
+        dp = torch.empty(n, dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        _check(self._L.cp_random_boxes(self._h, family, seed, max_label, n, _ptr(lo), _ptr(hi), _ptr(dp)),
+               "cp_random_boxes")
+        return lo, hi, dp
 
     def refine_resume(self) -> dict:
         """Continues the refinement interrupted by interrupt() (or loaded from a checkpoint)."""
@@ -446,6 +462,7 @@ def _declare_model(L):
     L.cp_model_loss_grad.argtypes = [I, P, P, P, P, SZ, P, P]
     L.cp_model_predict.argtypes = [P, I, P, P, P, SZ, P, P, P]
     L.cp_model_set_inference.argtypes = [P, I]
+    L.cp_model_set_wait_limit.argtypes = [P, ctypes.c_int32]
 
 
 def model_param_count() -> int:
@@ -512,6 +529,11 @@ class _ModelMixin:
         _declare_model(self._L)
         _check(self._L.cp_model_set_inference(self._h, kind), "cp_model_set_inference")
 
+    def model_set_wait_limit(self, polls):
+        """Polls per bounded completion wait of the tcgen05 inference kernel (0: every wait times out)."""
+        _declare_model(self._L)
+        _check(self._L.cp_model_set_wait_limit(self._h, polls), "cp_model_set_wait_limit")
+
     def model_predict(self, family, lo, hi, depth=None):
         _declare_model(self._L)
         lo = np.ascontiguousarray(lo, np.float64)
@@ -527,7 +549,7 @@ class _ModelMixin:
 
 
 for _name in ("model_collect", "model_records", "model_train", "model_params", "model_set_params", "model_predict",
-              "model_set_inference"):
+              "model_set_inference", "model_set_wait_limit"):
     setattr(Prover, _name, getattr(_ModelMixin, _name))
 
 
@@ -553,12 +575,17 @@ def lambda_shard(rank: int, world: int, lo: float = LAMBDA_MIN, hi: float = LAMB
 
 def reduce_report(report: dict, group=None) -> dict:
     """Sums a refinement report's counts over the ranks of a torch.distributed
-    group (any backend); times become the maximum over ranks."""
+    group (any backend): the scalar counts, the verdict histogram, the launches
+    and the per-depth histogram (padded to 64 depths, the report's bins);
+    max_depth_seen is recomputed from the summed histogram and the times become
+    the maximum over ranks.  Every rank must call it (two all-reduces)."""
     import torch
     import torch.distributed as dist
 
-    keys = ("evaluated", "unresolved", "clipped", "fp32_decided", "handles_evaluated")
-    v = torch.tensor([report[k] for k in keys] + list(report["verdicts"]), dtype=torch.float64)
+    keys = ("evaluated", "unresolved", "clipped", "fp32_decided", "handles_evaluated", "launches")
+    depth = list(report["per_depth"])[:64]
+    depth += [0] * (64 - len(depth))
+    v = torch.tensor([report[k] for k in keys] + list(report["verdicts"]) + depth, dtype=torch.float64)
     t = torch.tensor([report["device_ms"], report["wall_ms"]], dtype=torch.float64)
     if dist.get_backend(group) == "nccl":
         v, t = v.cuda(), t.cuda()
@@ -568,6 +595,11 @@ def reduce_report(report: dict, group=None) -> dict:
     out = dict(report)
     for i, k in enumerate(keys):
         out[k] = int(v[i])
-    out["verdicts"] = [int(x) for x in v[len(keys):]]
+    nk = len(keys)
+    out["verdicts"] = [int(x) for x in v[nk:nk + 5]]
+    hist = [int(x) for x in v[nk + 5:nk + 5 + 64]]
+    seen = max((d for d, c in enumerate(hist) if c), default=0)
+    out["per_depth"] = hist[: seen + 1]
+    out["max_depth_seen"] = seen
     out["device_ms"], out["wall_ms"] = t
     return out

@@ -83,6 +83,47 @@ __global__ void k_copy_seed(int dims, const double* __restrict__ lo, const doubl
     }
 }
 
+// Seeded random boxes on the family's domain (the uneven-depth workload of the
+// persistent engine).  Box i draws its numbers from a counter-based generator:
+// u(i, k) = top 53 bits of mix64(seed ^ mix64(8 i + k)) / 2^53.  Lambda has its
+// centre uniform in [0.5, 0.99]; each radius has its centre uniform in the
+// dependent range of the axes before it (the ranges the lattice enumerates,
+// with the single-placement table's upper bound); every axis has a log-uniform
+// width in [2^-20, 2^-4] and is intersected with its range.  A box whose range
+// is empty is marked dropped (depth 0xFF); the others get a depth label
+// uniform in 0..max_label.
+__device__ __forceinline__ double rand_unit(unsigned long long seed, unsigned long long i, int k) {
+    const unsigned long long z = mix64(seed ^ mix64(8ull * i + (unsigned long long)k));
+    return (double)(z >> 11) * 0x1.0p-53;
+}
+__device__ __forceinline__ bool rand_axis(unsigned long long seed, unsigned long long i, int k, Iv range, double* lo,
+                                          double* hi) {
+    if (!(range.lo <= range.hi)) return false;
+    const double c = range.lo + (range.hi - range.lo) * rand_unit(seed, i, k);
+    const double w = exp2(-20.0 + 16.0 * rand_unit(seed, i, k + 1));
+    *lo = fmax(range.lo, c - 0.5 * w);
+    *hi = fmin(range.hi, c + 0.5 * w);
+    return *lo <= *hi;
+}
+__global__ void k_random_boxes(int fam, unsigned long long seed, int max_label, size_t n, SingleTable tab, BoxList out) {
+    const int D = family_dims(fam);
+    const size_t step = (size_t)gridDim.x * blockDim.x;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += step) {
+        double l[4] = {0, 0, 0, 0}, h[4] = {0, 0, 0, 0};
+        bool alive = rand_axis(seed, t, 0, Iv{kLambdaMin, kLambdaMax}, &l[0], &h[0]);
+        const Iv la{l[0], h[0]};
+        if (alive) alive = rand_axis(seed, t, 2, range_r1(la, single_upper(tab, la.lo)), &l[1], &h[1]);
+        if (alive) alive = rand_axis(seed, t, 4, range_r2(fam, la, Iv{l[1], h[1]}), &l[2], &h[2]);
+        if (alive && D == 4) alive = rand_axis(seed, t, 6, range_r3(fam, la, Iv{l[2], h[2]}), &l[3], &h[3]);
+        for (int d = 0; d < D; ++d) {
+            out.lo[d * out.cap + t] = l[d];
+            out.hi[d * out.cap + t] = h[d];
+        }
+        const int label = (int)(rand_unit(seed, t, 8) * (double)(max_label + 1));
+        out.depth[t] = alive ? (uint8_t)(label > max_label ? max_label : label) : (uint8_t)0xFF;
+    }
+}
+
 __global__ void k_single_table(double lo, double h, int n, double* t, double* v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double x = __fma_rn((double)i, h, lo);
@@ -275,6 +316,9 @@ struct cp_prover {
     bool pending = false;
     cp_refine_opts pending_opts{};
     int variant[6][2] = {{1, 1}, {0, 0}, {1, 1}, {1, 1}, {0, 0}, {1, 1}};  // level-kernel variant per family/precision
+    // called before every lattice launch of cp_prove_family_reference
+    cp_step_callback step_cb = nullptr;
+    void* step_user = nullptr;
 };
 
 cudaStream_t cp_prover_stream(cp_prover* p) { return p->stream; }
@@ -409,6 +453,7 @@ cp_status cp_engine_launch_level(int fam, int prec, int variant, const BoxList& 
     a.max_depth = out ? max_depth : 0;
     a.axis_hint = nullptr;
     a.order_hint = nullptr;
+    a.digest = 0;
     cudaError_t e = cudaMemcpyAsync(counters + C_OUT, &out_base, sizeof(out_base), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cp_record_cuda_error(e, CP_ERR_CUDA);
     LevelKernel k = level_kernel(fam, prec, variant);
@@ -429,6 +474,8 @@ void cp_engine_fill_report(const unsigned long long* h, cp_refine_report* r) {
     r->clipped = (int64_t)h[C_CLIPPED];
     r->fp32_decided = (int64_t)h[C_FP32];
     r->handles_evaluated = (int64_t)h[C_HANDLES];
+    r->digest[0] = (uint64_t)h[C_DIGEST];
+    r->digest[1] = (uint64_t)h[C_DIGEST + 1];
     r->evaluated = 0;
     for (int v = 0; v < 5; ++v) r->evaluated += r->verdicts[v];
     r->max_depth_seen = 0;
@@ -455,6 +502,7 @@ cp_status cp_engine_eval_chunk(cp_prover* p, int fam, const cp_refine_opts& o, L
     a.max_depth = out ? o.max_depth : 0;
     a.axis_hint = axis_hint;
     a.order_hint = order_hint;
+    a.digest = o.digest ? 1 : 0;
     // children append after the boxes already in `out`
     unsigned long long base = out ? out->n : 0;
     CP_TRY(cuda_ok(cudaMemcpyAsync(p->cnt + C_OUT, &base, sizeof(base), cudaMemcpyHostToDevice, p->stream)));
@@ -522,20 +570,9 @@ cp_status refine_levels(cp_prover* p, const cp_refine_opts& o, cp_refine_report*
         }
     }
     (void)D;
+    cp_engine_fill_report(p->h_cnt, r);
     r->launches = launches;
     r->device_ms = ms;
-    for (int v = 0; v < 5; ++v) r->verdicts[v] = (int64_t)p->h_cnt[C_VERDICT + v];
-    r->unresolved = (int64_t)p->h_cnt[C_UNRESOLVED];
-    r->clipped = (int64_t)p->h_cnt[C_CLIPPED];
-    r->fp32_decided = (int64_t)p->h_cnt[C_FP32];
-    r->handles_evaluated = (int64_t)p->h_cnt[C_HANDLES];
-    r->evaluated = 0;
-    for (int v = 0; v < 5; ++v) r->evaluated += r->verdicts[v];
-    r->max_depth_seen = 0;
-    for (int d = 0; d < kDepthBins; ++d) {
-        r->per_depth[d] = (int64_t)p->h_cnt[C_COUNT + d];
-        if (r->per_depth[d]) r->max_depth_seen = d;
-    }
     r->wall_ms = now_ms() - t_wall0;
     return CP_OK;
 }
@@ -595,6 +632,7 @@ cp_status build_graph(cp_prover* p, const cp_refine_opts& o, int variant, int bp
         pa.bpt = bpt;
         pa.axis_hint = axis;
         pa.order_hint = order;
+        pa.digest = o.digest ? 1 : 0;
         void* kern = prec ? cp_graph_kernel_fp32(fam, variant) : cp_graph_kernel_fp64(fam, variant);
         const int block = kGraphBlock[variant];
         int per_sm = 0, sms = 148;
@@ -646,7 +684,7 @@ cp_status refine_graph(cp_prover* p, const cp_refine_opts& o, cp_refine_report* 
     const unsigned long long key[12] = {ls_bits, (unsigned long long)fam + 1, (unsigned long long)prec, (unsigned long long)variant,
                                         (unsigned long long)bpt, (unsigned long long)o.policy,
                                         (unsigned long long)o.max_depth,
-                                        (unsigned long long)(learned_axis | (learned_order << 1)),
+                                        (unsigned long long)(learned_axis | (learned_order << 1) | (o.digest ? 4 : 0)),
                                         (unsigned long long)(uintptr_t)p->levels[0].b.lo, (unsigned long long)p->level_cap,
                                         (unsigned long long)nlevels,
                                         (unsigned long long)(uintptr_t)cp_model_hint_buffer(p)};
@@ -756,10 +794,17 @@ void cp_request_interrupt(cp_prover* p) {
     if (p) p->interrupt.store(1);
 }
 
+void cp_set_step_callback(cp_prover* p, cp_step_callback cb, void* user) {
+    if (!p) return;
+    p->step_cb = cb;
+    p->step_user = user;
+}
+
 cp_status cp_refine(cp_prover* p, const cp_refine_opts* o, cp_refine_report* r) {
     if (!p || !r) return CP_ERR_INVALID;
     CP_TRY(check_opts(o));
     p->pending = false;
+    p->interrupt.store(0);  // a request made while no refinement ran does not stop this one
     const double t0 = now_ms();
     std::memset(r, 0, sizeof(*r));
     CP_TRY(cuda_ok(cudaSetDevice(p->device)));
@@ -783,6 +828,19 @@ cp_status cp_refine(cp_prover* p, const cp_refine_opts* o, cp_refine_report* r) 
     p->levels[0].n = total;
     CP_TRY(reset_counters(p));
     return run_refinement(p, *o, r, t0);
+}
+
+cp_status cp_random_boxes(cp_prover* p, int family, uint64_t seed, int max_label, size_t n, double* lo, double* hi,
+                          uint8_t* depth) {
+    if (!p || family < 0 || family > 5 || max_label < 0 || max_label > 250 || (n && (!lo || !hi || !depth)))
+        return CP_ERR_INVALID;
+    if (!n) return CP_OK;
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    const BoxList out{lo, hi, depth, n};
+    k_random_boxes<<<grid_of(k_random_boxes, 128), 128, 0, p->stream>>>(family, (unsigned long long)seed, max_label, n,
+                                                                        table_of(p), out);
+    CP_TRY(cp_check_launch());
+    return cuda_ok(cudaStreamSynchronize(p->stream));
 }
 
 cp_status cp_set_level_variant(cp_prover* p, int family, int precision, int variant) {
@@ -849,6 +907,7 @@ cp_status cp_refine_boxes(cp_prover* p, const cp_refine_opts* o, const double* l
     if (!p || !r || (n && (!lo || !hi))) return CP_ERR_INVALID;
     CP_TRY(check_opts(o));
     p->pending = false;
+    p->interrupt.store(0);  // a request made while no refinement ran does not stop this one
     const double t0 = now_ms();
     std::memset(r, 0, sizeof(*r));
     CP_TRY(cuda_ok(cudaSetDevice(p->device)));
@@ -873,6 +932,7 @@ cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* o, const doub
     if (!p || !r || (n && (!lo || !hi))) return CP_ERR_INVALID;
     CP_TRY(check_opts(o));
     p->pending = false;
+    p->interrupt.store(0);  // a request made while no refinement ran does not stop this one
     const double t0 = now_ms();
     std::memset(r, 0, sizeof(*r));
     CP_TRY(cuda_ok(cudaSetDevice(p->device)));
@@ -1112,6 +1172,7 @@ cp_status cp_prove_family_reference(cp_prover* p, int family, double la_lb, doub
         }
         const auto cur = q.top();
         q.pop();
+        if (p->step_cb) p->step_cb(p->step_user, cur.first, cur.second);
         double first = INFINITY;
         cudaEventRecord(e0, p->stream);
         cp_status s = cp_reference_step(p, family, cur.first, cur.second, sizes, &first, nullptr);

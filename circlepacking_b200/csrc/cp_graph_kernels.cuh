@@ -24,6 +24,7 @@ struct PersistArgs {
     double lambda_scale;
     const uint8_t* axis_hint;   // per box of the job, indexed from job.begin
     const uint8_t* order_hint;
+    int digest;
 };
 
 // The chunk of the current job: warps claim 32 * bpt consecutive boxes at a
@@ -47,6 +48,7 @@ __global__ void __launch_bounds__(BLOCK) __maxnreg__(graph_regs(BLOCK)) k_level_
     a.max_depth = job.out_level >= 0 ? pa.max_depth : 0;
     a.axis_hint = pa.axis_hint;
     a.order_hint = pa.order_hint;
+    a.digest = pa.digest;
     level_smem_init(sm);
     __syncthreads();
     unsigned handles = 0;

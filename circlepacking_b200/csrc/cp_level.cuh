@@ -29,7 +29,8 @@ enum : int {
     C_NOFIT_SLAB = 23,  // smallest lambda slab holding a box whose fit check fired (middle/end)
     C_TRAP_SLAB = 24,   // smallest lambda slab holding a box that reached a trap site
     C_HANDLES = 25,     // guarded criteria evaluated in FP64
-    C_COUNT = 26
+    C_DIGEST = 26,      // 2 words: sum and xor of the per-box verdict hashes (when enabled)
+    C_COUNT = 28
 };
 enum : unsigned long long { E_OVERFLOW = 1, E_NOFIT = 2, E_TRAP = 4 };
 constexpr int kDepthBins = 64;
@@ -45,7 +46,30 @@ struct LevelArgs {
     double lambda_scale;        // SPLIT_HYBRID
     const uint8_t* axis_hint;   // per input box (SPLIT_GIVEN), indexed from `begin`
     const uint8_t* order_hint;  // per input box criterion order, or null
+    int digest;                 // 1: fold every evaluated (box, verdict) pair into the digest counters
 };
+
+// Order-independent digest of a set of (box, verdict) pairs: each evaluated box
+// contributes a 64-bit hash of the bit patterns of its bounds and its verdict,
+// summed (mod 2^64) and, after a second finalisation, xor-ed into two counters.
+// Two refinements that evaluate the same boxes with the same verdicts give the
+// same pair of words in any order.  The mixing step is the splitmix64 finaliser
+// (Steele, Lea and Flood, "Fast splittable pseudorandom number generators", 2014).
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+template <int D>
+__device__ __forceinline__ unsigned long long box_hash(const double* lo, const double* hi, int verdict) {
+    unsigned long long h = 0x9e3779b97f4a7c15ull * (unsigned long long)(verdict + 1);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        h = mix64(h ^ (unsigned long long)__double_as_longlong(lo[d]));
+        h = mix64(h + (unsigned long long)__double_as_longlong(hi[d]));
+    }
+    return h;
+}
 
 // Per-block shared state of the level step; WARPS = warps per block.
 template <int WARPS>
@@ -53,6 +77,7 @@ struct LevelSmem {
     unsigned long long hist[8];
     unsigned long long depth[kDepthBins];
     unsigned long long handles;
+    unsigned long long dig_sum, dig_xor;
     // per warp: the lane owning each slot of one iteration's children
     uint8_t own[WARPS][32 * 16];
 };
@@ -61,7 +86,11 @@ template <int WARPS>
 __device__ __forceinline__ void level_smem_init(LevelSmem<WARPS>& sm) {
     for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x) sm.depth[t] = 0;
     if (threadIdx.x < 8) sm.hist[threadIdx.x] = 0;
-    if (threadIdx.x == 0) sm.handles = 0;
+    if (threadIdx.x == 0) {
+        sm.handles = 0;
+        sm.dig_sum = 0;
+        sm.dig_xor = 0;
+    }
 }
 
 // One lane's box j of the chunk (j >= a.count: the lane only takes part in the
@@ -103,6 +132,11 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
             }
             atomicAdd(&sm.hist[v], 1ull);
             atomicAdd(&sm.depth[depth < kDepthBins ? depth : kDepthBins - 1], 1ull);
+            if (a.digest) {
+                const unsigned long long h = box_hash<D>(lo, hi, v);
+                atomicAdd(&sm.dig_sum, h);
+                atomicXor(&sm.dig_xor, mix64(h ^ 0x5851f42d4c957f2dull));
+            }
             if (v != V_PROVED && v != V_EMPTY) {
                 if (depth >= a.max_depth) {
                     atomicAdd(&sm.hist[C_UNRESOLVED], 1ull);
@@ -170,6 +204,10 @@ __device__ __forceinline__ void level_flush(const LevelArgs& a, LevelSmem<WARPS>
     if (threadIdx.x < 8 && threadIdx.x != C_OUT && sm.hist[threadIdx.x])
         atomicAdd(&a.cnt[threadIdx.x], sm.hist[threadIdx.x]);
     if (threadIdx.x == 0 && sm.handles) atomicAdd(&a.cnt[C_HANDLES], sm.handles);
+    if (threadIdx.x == 0 && a.digest) {
+        atomicAdd(&a.cnt[C_DIGEST], sm.dig_sum);
+        atomicXor(&a.cnt[C_DIGEST + 1], sm.dig_xor);
+    }
     for (int t = threadIdx.x; t < kDepthBins; t += blockDim.x)
         if (sm.depth[t]) atomicAdd(&a.per_depth[t], sm.depth[t]);
 }

@@ -673,8 +673,9 @@ __device__ __forceinline__ void tc_commit(uint32_t mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                  : "memory");
 }
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-    for (int it = 0; it < (1 << 22); ++it) {
+constexpr int kTcWaitLimit = 1 << 22;  // default polls of a bounded completion wait
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, int limit = kTcWaitLimit) {
+    for (int it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
@@ -702,7 +703,8 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t* r) {
 
 struct TcArgs {
     InferArgs a;
-    int* err;  // raised when an MMA-completion wait times out
+    int* err;        // raised when an MMA-completion wait times out
+    int wait_limit;  // polls per completion wait (0: every wait times out at once)
 };
 
 template <int FAM>
@@ -788,8 +790,10 @@ __global__ void __launch_bounds__(kTcRows) k_infer_tc(TcArgs ta) {
                 }
                 tc_commit(mbar);
             }
-            ok = __syncthreads_and(mbar_wait(mbar, phase) ? 1 : 0) != 0;  // block-uniform
-            phase ^= 1u;
+            ok = __syncthreads_and(mbar_wait(mbar, phase, ta.wait_limit) ? 1 : 0) != 0;  // block-uniform
+            // the parity advances only past a completed phase: after a time-out
+            // `phase` still names the pending one, which the drain below waits for
+            if (ok) phase ^= 1u;
             tc_fence_after();
             if (!ok) break;
             if (layer < 2) {
@@ -830,7 +834,9 @@ __global__ void __launch_bounds__(kTcRows) k_infer_tc(TcArgs ta) {
     }
     if (!ok) {
         if (tid == 0) atomicExch(ta.err, 1);
-        mbar_wait(mbar, phase);  // bounded: let an MMA still in flight finish before freeing its memory
+        // bounded: let the MMA still in flight (committed to the pending phase)
+        // finish before its tensor memory is freed
+        mbar_wait(mbar, phase);
     }
     tc_fence_before();
     __syncthreads();
@@ -964,6 +970,7 @@ struct ModelState {
     int infer_kind = 0;
     int* tc_err = nullptr;    // device flag raised by a timed-out tcgen05 wait
     int* tc_err_h = nullptr;  // pinned copy, refreshed after every tcgen05 launch
+    int tc_wait_limit = kTcWaitLimit;
     // per-chunk hints
     uint8_t* hint_axis = nullptr;
     uint8_t* hint_order = nullptr;
@@ -1149,6 +1156,7 @@ cp_status run_infer(ModelState* m, int fam, const InferArgs& a, cudaStream_t st)
     TcArgs t;
     t.a = a;
     t.err = m->tc_err;
+    t.wait_limit = m->tc_wait_limit;
     M_TRY(launch_infer_tc(fam, t, st));
     return ok_or(cudaMemcpyAsync(m->tc_err_h, m->tc_err, sizeof(int), cudaMemcpyDeviceToHost, st));
 }
@@ -1509,7 +1517,22 @@ cp_status cp_model_predict(cp_prover* p, int family, const double* lo, const dou
 
 cp_status cp_model_set_inference(cp_prover* p, int kind) {
     if (!p || kind < 0 || kind > 1) return cp_fail(CP_ERR_INVALID, "cp_model_set_inference: kind 0 or 1");
-    state(p, true)->infer_kind = kind;
+    ModelState* m = state(p, true);
+    m->infer_kind = kind;
+    // a time-out recorded by an earlier tcgen05 launch is cleared
+    if (m->tc_err) {
+        cudaStream_t st = cp_prover_stream(p);
+        M_TRY(ok_or(cudaStreamSynchronize(st)));
+        M_TRY(ok_or(cudaMemsetAsync(m->tc_err, 0, sizeof(int), st)));
+        M_TRY(ok_or(cudaStreamSynchronize(st)));
+        *m->tc_err_h = 0;
+    }
+    return CP_OK;
+}
+
+cp_status cp_model_set_wait_limit(cp_prover* p, int32_t polls) {
+    if (!p || polls < 0) return cp_fail(CP_ERR_INVALID, "cp_model_set_wait_limit: polls >= 0");
+    state(p, true)->tc_wait_limit = polls;
     return CP_OK;
 }
 

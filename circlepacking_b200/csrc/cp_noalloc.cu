@@ -79,10 +79,20 @@ extern "C" cp_status cp_refine_boxes_static(int family, int precision, int polic
                        CP_STATIC_MAX_SEEDS, CP_STATIC_MAX_DEPTH, n, max_depth);
     }
     std::memset(report, 0, sizeof(*report));
+    // the host mirror of the counter block below is a fixed-size local array
+    const size_t words = cp_engine_counter_words();
+    if (words > 128) return cp_fail(CP_ERR_INVALID, "cp_refine_boxes_static: counter block of %zu words", words);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) return cp_record_cuda_error(e, CP_ERR_NO_DEVICE);
     cudaStream_t st = (cudaStream_t)stream;
+    // the scratch array resolved below belongs to the current device: a stream
+    // of another device would run kernels on memory it cannot address
+    int stream_dev = dev;
+    if ((e = cudaStreamGetDevice(st, &stream_dev)) != cudaSuccess) return cp_record_cuda_error(e, CP_ERR_CUDA);
+    if (stream_dev != dev)
+        return cp_fail(CP_ERR_INVALID, "cp_refine_boxes_static: the stream belongs to device %d, the current device is %d",
+                       stream_dev, dev);
     unsigned char* base = nullptr;
     cp_status rc = setup(dev, st, &base);
     if (rc != CP_OK) return rc;
@@ -115,7 +125,6 @@ extern "C" cp_status cp_refine_boxes_static(int family, int precision, int polic
         p += bytes;
     }
     // the counters must start at zero; the level buffers are written before read
-    const size_t words = cp_engine_counter_words();
     if ((e = cudaMemsetAsync(cnt, 0, words * sizeof(unsigned long long), st)) != cudaSuccess)
         return cp_record_cuda_error(e, CP_ERR_CUDA);
     for (int d = 0; d < D && n; ++d) {
@@ -132,7 +141,6 @@ extern "C" cp_status cp_refine_boxes_static(int family, int precision, int polic
     }
     cnt_in[0] = n;
     unsigned long long h_cnt[128] = {0};
-    if (words > 128) return CP_ERR_INVALID;
     // deepest non-empty level first, in chunks whose children fit the next level
     for (;;) {
         int l = -1;

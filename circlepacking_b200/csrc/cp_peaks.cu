@@ -28,6 +28,7 @@ __global__ void __launch_bounds__(256) k_probe(double seed, double* out) {
             if (OP == 4) x[c] = asin(x[c]) * 0.5 + 0.25;
             if (OP == 5) x[c] = cpb::div_rd(x[c], 1.0000001);
             if (OP == 6) x[c] = cpb::div_dir<false, 1>(x[c], 1.0000001);
+            if (OP == 7) x[c] = cpb::div_dir<false, 0>(x[c], 1.0000001);
         }
     }
     double s = 0;
@@ -87,6 +88,7 @@ extern "C" cp_status cp_measure_primitives(int device, double* rates) {
     rates[5] = rate_of(k_probe_ffma, 0.5f, out, grid, block, 20);
     rates[6] = rate_of(k_probe<5>, 0.5, out, grid, block, 4);
     rates[7] = rate_of(k_probe<6>, 0.5, out, grid, block, 4);
+    rates[8] = rate_of(k_probe<7>, 0.5, out, grid, block, 4);
     cudaFree(out);
     return cp_check_launch();
 }

@@ -11,14 +11,18 @@
 //   run_kernel.cuh:36-132            the lambda loop and its SIGINT handling
 //
 // Each family runs cp_prove_family_reference over [lambda_min, lambda_max] with
-// the reference's lattice sizes.  On SIGINT the first remaining lambda interval is
-// rerun once and its failing boxes are printed in the reference's format
-// (e.g. middle_configuration.cu:181-183); a second SIGINT ends the process as the
-// reference's handler does.
+// the reference's lattice sizes, printing "Handling lambda interval [lb, ub]" to
+// stderr before every launch as run_kernel.cuh:79 does.  On SIGINT the first
+// remaining lambda interval is rerun once and its failing boxes are printed in
+// the reference's format (e.g. middle_configuration.cu:181-183,
+// end_configuration.cu:124); a second SIGINT ends the process as the reference's
+// handler does.  The reference prints every failing box; the environment
+// variable CP_CRITICALS_MAX (default 1048576) bounds the lines printed here.
 #include <csignal>
 #include <cstddef>
 #include <cstdio>
 #include <cstdlib>
+#include <iomanip>
 #include <iostream>
 #include <stdexcept>
 #include <string>
@@ -52,7 +56,10 @@ cp_prover* handle() {
     return h;
 }
 
-// the labels of the reference's critical-interval lines, per family and handle
+// The label of the reference's critical-interval lines, per family and handle,
+// and the separator before "la = ": ": " in start_configuration.cu:147,158,207 and
+// middle_configuration.cu:182,193; " - " in start_configuration.cu:289 and
+// end_configuration.cu:124,135,245,256.
 const char* label(int family, int handle_bit) {
     switch (family) {
     case CP_START: return handle_bit == 0 ? "Critical interval: Start configuration, case 1" : "Critical interval: Start configuration, case 2";
@@ -63,26 +70,51 @@ const char* label(int family, int handle_bit) {
     default: return handle_bit == 0 ? "End configuration (3 disks): Critical interval with r1 on the inside" : "End configuration (3 disks): Critical interval with r1 on the outside";
     }
 }
+const char* separator(int family) {
+    return (family == CP_START_END_3D || family == CP_END_2D || family == CP_END_3D) ? " - " : ": ";
+}
+
+size_t criticals_max() {
+    const char* e = std::getenv("CP_CRITICALS_MAX");
+    if (!e || !*e) return size_t(1) << 20;
+    char* end = nullptr;
+    const unsigned long long v = std::strtoull(e, &end, 10);
+    return (end && *end == '\0') ? (size_t)v : (size_t(1) << 20);
+}
 
 void print_criticals(cp_prover* p, int family, double lb, double ub) {
-    const size_t cap = 1u << 20;
-    std::vector<double> boxes(8 * cap);
-    std::vector<uint8_t> handles(cap);
+    const size_t cap = criticals_max();
+    std::vector<double> boxes(8 * (cap ? cap : 1));
+    std::vector<uint8_t> handles(cap ? cap : 1);
     size_t count = 0;
     if (cp_reference_criticals(p, family, lb, ub, nullptr, cap, boxes.data(), handles.data(), &count) != CP_OK) return;
     const int dims = cp_family_dims(family);
+    const char* sep = separator(family);
     for (size_t i = 0; i < count && i < cap; ++i) {
         const double* b = &boxes[8 * i];
         for (int h = 0; h < 2; ++h) {
             if (!((handles[i] >> h) & 1)) continue;
             if (dims == 4)
-                std::printf("%s: la = [%.19g,%.19g], r1 = [%.19g,%.19g], r2 = [%.19g,%.19g], r3 = [%.19g,%.19g]\n",
-                            label(family, h), b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7]);
+                std::printf("%s%sla = [%.19g,%.19g], r1 = [%.19g,%.19g], r2 = [%.19g,%.19g], r3 = [%.19g,%.19g]\n",
+                            label(family, h), sep, b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7]);
             else
-                std::printf("%s: la = [%.19g,%.19g], r1 = [%.19g,%.19g], r2 = [%.19g,%.19g]\n", label(family, h), b[0],
-                            b[1], b[2], b[3], b[4], b[5]);
+                std::printf("%s%sla = [%.19g,%.19g], r1 = [%.19g,%.19g], r2 = [%.19g,%.19g]\n", label(family, h), sep,
+                            b[0], b[1], b[2], b[3], b[4], b[5]);
         }
     }
+    std::fflush(stdout);
+}
+
+// "Handling lambda interval " followed by the interval as the reference's
+// operator<< writes it (interval.hpp:295-303): right-aligned fields of width 26,
+// 19 significant digits.
+void on_step(void*, double lb, double ub) {
+    const std::ios_base::fmtflags flags = std::cerr.flags(std::ios::right);
+    const std::streamsize prec = std::cerr.precision(19);
+    std::cerr << "Handling lambda interval " << '[' << std::setw(26) << lb << ", " << std::setw(26) << ub << ']'
+              << std::endl;
+    std::cerr.flags(flags);
+    std::cerr.precision(prec);
 }
 
 // run_kernel_until_no_criticals for one family; true when the lambda queue emptied
@@ -91,9 +123,11 @@ bool run_family(int family) {
     g_interrupts = 0;
     g_active = p;
     g_previous = std::signal(SIGINT, on_sigint);
+    cp_set_step_callback(p, on_step, nullptr);
     cp_reference_report r;
     const cp_status s = cp_prove_family_reference(p, family, kLambdaMin, kLambdaMax, nullptr, 0, nullptr, &r);
     std::signal(SIGINT, g_previous);
+    cp_set_step_callback(p, nullptr, nullptr);
     g_active = nullptr;
     if (s == CP_ERR_INTERRUPTED) {
         std::cerr << "We were interrupted - running the first remaining interval with output once!" << std::endl;

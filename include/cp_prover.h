@@ -161,6 +161,12 @@ void* cp_get_stream(cp_prover* p);
  * from a signal handler or another thread. */
 void cp_request_interrupt(cp_prover* p);
 
+/* Called by cp_prove_family_reference before each lattice launch with the
+ * lambda interval about to be handled (the reference writes that interval to
+ * stderr, run_kernel.cuh:79).  cb = NULL removes the callback. */
+typedef void (*cp_step_callback)(void* user, double la_lb, double la_ub);
+void cp_set_step_callback(cp_prover* p, cp_step_callback cb, void* user);
+
 /* Split policies for the box refinement. */
 typedef enum cp_split_policy {
     CP_SPLIT_UNIFORM = 0, /* bisect every axis (2^dims children) */
@@ -184,6 +190,7 @@ typedef struct cp_refine_opts {
     int32_t engine;         /* cp_engine: host-driven level loop or one CUDA graph launch */
     int32_t boxes_per_thread; /* graph engine: boxes a warp lane takes per claim (1..8); 0 = tuned */
     double lambda_scale;    /* CP_SPLIT_HYBRID: lambda target width scale; 0 = 4e-3 */
+    int32_t digest;         /* 1 = compute report->digest (per-box verdict identity checks) */
 } cp_refine_opts;
 
 /* Refinement engines.  CP_ENGINE_LEVELS: the host picks each chunk, launches
@@ -207,6 +214,11 @@ typedef struct cp_refine_report {
     double device_ms;        /* summed kernel time (CUDA events on the handle's stream) */
     double wall_ms;          /* host wall time of the call */
     int64_t handles_evaluated; /* guarded criteria evaluated in FP64 (DECIDE order) */
+    /* with opts->digest: an order-independent 64-bit sum and xor of a hash of
+     * every evaluated box's bounds (bit patterns) and verdict.  Two refinements
+     * with equal digests evaluated the same boxes with the same verdicts (up to
+     * a 2^-64 collision chance); 0 without opts->digest. */
+    uint64_t digest[2];
 } cp_refine_report;
 
 /* Refines a family's lattice seed until every box is proved / empty or reaches
@@ -260,6 +272,17 @@ cp_status cp_prove_family_reference(cp_prover* p, int family, double la_lb, doub
 cp_status cp_reference_criticals(cp_prover* p, int family, double la_lb, double la_ub, const int32_t* sizes,
                                  size_t max_boxes, double* boxes, uint8_t* handles, size_t* count);
 
+/* Seeded random boxes on a family's domain, for uneven-depth workloads of the
+ * refinement engine (no counterpart in the reference).  Box i takes its numbers
+ * from a counter-based generator keyed on (seed, i): lambda's centre is uniform
+ * in [0.5, 0.99]; each radius's centre is uniform in its dependent range given
+ * the axes before it; every axis has a log-uniform width in [2^-20, 2^-4] and is
+ * intersected with its range; the depth byte is uniform in 0..max_label, or
+ * 0xFF (dropped, counted as clipped by a refinement) when a range is empty.
+ * lo, hi: device SoA with stride n; depth: n device bytes.  Synchronous. */
+cp_status cp_random_boxes(cp_prover* p, int family, uint64_t seed, int max_label, size_t n, double* lo, double* hi,
+                          uint8_t* depth);
+
 /* As cp_refine_boxes with HOST seed buffers (lo/hi SoA with stride n): copies
  * the seeds into the handle's worklist, refines, synchronises. */
 cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* opts, const double* lo, const double* hi,
@@ -276,8 +299,9 @@ cp_status cp_div_check(const double* a, const double* b, size_t n, double* out, 
  * of the FP64 primitives the criteria use, each run alone with full occupancy
  * and independent chains: rates[0] DFMA, [1] __dadd_rd, [2] __dmul_rd,
  * [3] __ddiv_rd, [4] asin (CUDA libm), [5] FFMA (FP32), [6] the library's
- * directed division (cp_div_check), [7] the same seeded from the FP32
- * reciprocal (rates holds 8 doubles).  Synchronous. */
+ * directed division as the kernels call it (one shared copy, cp_div_check),
+ * [7] the same inlined and seeded from the FP32 reciprocal, [8] inlined with the
+ * FP64 reciprocal seed (rates holds 9 doubles).  Synchronous. */
 cp_status cp_measure_primitives(int device, double* rates);
 
 /* ---------------------------------------------------------------- resume and checkpoints
@@ -365,6 +389,13 @@ cp_status cp_model_loss_grad(int family, const float* params, const float* feats
  * 1 = tcgen05.mma with FP32 accumulators in tensor memory, 128 boxes per CTA
  * (bounded completion waits; a time-out returns CP_ERR_DEVICE). */
 cp_status cp_model_set_inference(cp_prover* p, int kind);
+
+/* Diagnostics: polls per bounded completion wait of the tcgen05 inference
+ * kernel (default 4194304).  0 makes every wait time out at once, so a test can
+ * reach the kernel's error path: it drains the MMA in flight, frees its tensor
+ * memory and the call returns CP_ERR_DEVICE.  cp_model_set_inference clears a
+ * recorded time-out. */
+cp_status cp_model_set_wait_limit(cp_prover* p, int32_t polls);
 
 /* Network outputs for host boxes (lo/hi SoA, stride n; depth may be NULL):
  * logits [n][8], the chosen split axis and criterion order per box. */

@@ -41,6 +41,11 @@ static thread_local OpCount* t_count = nullptr;
 
 // trap sites reached while evaluating the current box (reference: algcuda::trap)
 static thread_local bool t_trap = false;
+// Reference-kernel path (op counting only): stop at the first failing
+// sub-check of a handle and at the first failing handle of a box, and at the fit
+// check where the kernel traps (middle_configuration.cu:173-199,
+// end_configuration.cu:115-144, 236-265, start_configuration.cu:141-162).
+static thread_local bool t_decide = false;
 
 // ---------------------------------------------------------------- rounding
 static inline uint64_t bits_of(double x) {
@@ -589,7 +594,10 @@ static void middle_case(Iv la, Iv r1, Iv r2, Iv r3, Iv c12, Iv c13, Iv c23, Out&
         double lhs = mul_rd(0.5, add_rd(ar1, ar2));
         double rhs = mul_ru(kCriticalRatio, used);
         set_trace(o, k0, lhs, rhs);
-        if (lhs < rhs) o.mask |= (uint8_t)(1u << k0);
+        if (lhs < rhs) {
+            o.mask |= (uint8_t)(1u << k0);
+            if (t_decide) return;
+        }
     }
     if (possibly(unot(case_a))) {
         double used = mul_ru(ratio, mul_ru(0.5, c13.ub));
@@ -693,6 +701,7 @@ static void eval_box(int fam, const double* lo, const double* hi, Out& o) {
         if (possibly(case1)) {
             if (!start_case_1(la, r1, r2, a12, &lhs, &rhs)) o.mask |= 1;
             set_trace(o, 0, lhs, rhs);
+            if (t_decide && (o.mask & 1)) break;
         }
         if (possibly(unot(case1))) {
             if (!start_case_2(la, r1, r2, r3, a13, &lhs, &rhs)) o.mask |= 2;
@@ -710,25 +719,31 @@ static void eval_box(int fam, const double* lo, const double* hi, Out& o) {
         break;
     case MIDDLE: {
         if (fit_fires) o.mask |= M_FIT;
+        if (t_decide && fit_fires) break;
         Iv c12 = ca_inner_outer(la, r1, r2), c13 = ca_inner_inner(la, r1, r3), c23 = ca_outer_inner(la, r2, r3);
         middle_case(la, r1, r2, r3, c12, c13, c23, o, 0);
+        if (t_decide && (o.mask & 3)) break;
         Iv d12 = ca_outer_inner(la, r1, r2), d13 = ca_outer_outer(r1, r3), d23 = ca_inner_outer(la, r2, r3);
         middle_case(la, r1, r2, r3, d12, d13, d23, o, 2);
         break;
     }
     case END_2D:
         if (fit_fires) o.mask |= M_FIT;
+        if (t_decide && fit_fires) break;
         if (!end_inner_outer_2d(la, r1, r2, &lhs, &rhs)) o.mask |= 1;
         set_trace(o, 0, lhs, rhs);
+        if (t_decide && (o.mask & 1)) break;
         if (!end_outer_inner_2d(la, r1, r2, &lhs, &rhs)) o.mask |= 2;
         set_trace(o, 1, lhs, rhs);
         break;
     case END_3D: {
         if (fit_fires) o.mask |= M_FIT;
+        if (t_decide && fit_fires) break;
         for (int k = 0; k < 2; ++k) {
             int r = end_3d_case(k == 0, la, r1, r2, r3, &lhs, &rhs);
             if (r >= 0) set_trace(o, k, lhs, rhs);
             if (r == 0) o.mask |= (uint8_t)(1u << k);
+            if (t_decide && r == 0) break;
         }
         break;
     }
@@ -838,13 +853,17 @@ int orc_eval_boxes(int fam, const double* lo, const double* hi, int64_t n, int64
     return 0;
 }
 
-// Count the primitive operations of the reference's evaluation path over n
-// boxes.  counts[0..3] = add/sub, mul, div, asin (summed over the boxes).
-int orc_count_ops(int fam, const double* lo, const double* hi, int64_t n, int64_t stride, uint64_t* counts) {
+// Count the primitive operations of the evaluation of n boxes.
+// counts[0..3] = add/sub, mul, div, asin (summed over the boxes).  decide = 0:
+// every sub-criterion (FULL); decide = 1: the reference kernel's own path, which
+// stops at the first failing sub-check / handle and at a firing fit check.
+int orc_count_ops_mode(int fam, const double* lo, const double* hi, int64_t n, int64_t stride, int decide,
+                       uint64_t* counts) {
     if (fam < 0 || fam > 5 || n < 0) return 1;
     const int dims = family_dims(fam);
     OpCount c{0, 0, 0, 0};
     t_count = &c;
+    t_decide = decide != 0;
     double l[4], h[4];
     Out o;
     for (int64_t i = 0; i < n; ++i) {
@@ -855,11 +874,15 @@ int orc_count_ops(int fam, const double* lo, const double* hi, int64_t n, int64_
         eval_box(fam, l, h, o);
     }
     t_count = nullptr;
+    t_decide = false;
     counts[0] = c.add;
     counts[1] = c.mul;
     counts[2] = c.div;
     counts[3] = c.asin;
     return 0;
+}
+int orc_count_ops(int fam, const double* lo, const double* hi, int64_t n, int64_t stride, uint64_t* counts) {
+    return orc_count_ops_mode(fam, lo, hi, n, stride, 0, counts);
 }
 
 double orc_single_placement(double lb_lambda) { return single_placement(lb_lambda); }

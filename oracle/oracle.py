@@ -42,6 +42,7 @@ def lib():
         P, I64, I32, D = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double
         L.orc_eval_boxes.argtypes = [I32, P, P, I64, I64, P, P, P, I32]
         L.orc_count_ops.argtypes = [I32, P, P, I64, I64, P]
+        L.orc_count_ops_mode.argtypes = [I32, P, P, I64, I64, I32, P]
         L.orc_single_placement.argtypes = [D]
         L.orc_single_placement.restype = D
         L.orc_asin_pad.argtypes = [P, I64, P, P]
@@ -76,11 +77,14 @@ def eval_boxes(family: int, lo: np.ndarray, hi: np.ndarray, trace: bool = False,
     return (v, m, t) if trace else (v, m)
 
 
-def count_ops(family: int, lo: np.ndarray, hi: np.ndarray) -> dict:
+def count_ops(family: int, lo: np.ndarray, hi: np.ndarray, decide: bool = False) -> dict:
+    """Primitive operations (add/sub, mul, div, asin) of evaluating boxes lo/hi:
+    every sub-criterion (decide=False), or the reference kernel's own path, which
+    stops at the first failing sub-check and handle (decide=True)."""
     lo = np.ascontiguousarray(lo, dtype=np.float64)
     hi = np.ascontiguousarray(hi, dtype=np.float64)
     c = np.zeros(4, np.uint64)
-    lib().orc_count_ops(family, _p(lo), _p(hi), lo.shape[1], lo.shape[1], _p(c))
+    lib().orc_count_ops_mode(family, _p(lo), _p(hi), lo.shape[1], lo.shape[1], int(decide), _p(c))
     return dict(add=int(c[0]), mul=int(c[1]), div=int(c[2]), asin=int(c[3]), boxes=int(lo.shape[1]))
 
 

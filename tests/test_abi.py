@@ -63,8 +63,9 @@ def test_invalid_arguments_rejected_without_device(libpath):
 def test_reference_prover_links_against_shim(libpath, tmp_path):
     """The reference's own prover.cpp links unchanged against the library (the
     C++ shim defines circlepacking::lane_packing::find_critical_intervals)."""
-    ref = "/root/reference/code"
-    if not os.path.exists(os.path.join(ref, "prover.cpp")):
+    ref = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref-dir"], capture_output=True,
+                         text=True).stdout.strip()
+    if not ref or not os.path.exists(os.path.join(ref, "prover.cpp")):
         pytest.skip("reference sources not present on this machine")
     out = tmp_path / "prover_b200"
     libdir = os.path.dirname(libpath)

@@ -142,3 +142,50 @@ def test_tcgen05_inference_matches_mma_sync(cp, oracle, prover, family):
     want = np.abs(np.maximum(l0[:, 2], l0[:, 3]) - np.maximum(l0[:, 0], l0[:, 1])) > 1e-3 if family == 3 else \
         np.abs(l0[:, 1] - l0[:, 0]) > 1e-3
     assert (o1 == o0)[want].all()
+
+
+@pytest.mark.parametrize("family", [3, 0])
+def test_tcgen05_inference_matches_oracle(cp, oracle, prover, family):
+    """The tcgen05 inference kernel against the CPU restatement of the network
+    (oracle/mlp.py): logits within the BF16 tolerance of the mma.sync test."""
+    params = mlp.init_params(41 + family)
+    prover.model_set_params(family, params)
+    dims = boxgen.DIMS[family]
+    idx = boxgen.lattice_indices(family, [64, 16, 16, 8][:dims], 3000, 23)
+    lo, hi = oracle.lattice_boxes(family, boxgen.LAMBDA, [64, 16, 16, 8][:dims], idx)
+    lo, hi = boxgen.sub_boxes(lo, hi, 24)
+    depth = np.random.default_rng(25).integers(0, 30, lo.shape[1]).astype(np.uint8)
+    try:
+        prover.model_set_inference(1)
+        logits, axis, _ = prover.model_predict(family, lo, hi, depth)
+    finally:
+        prover.model_set_inference(0)
+    want = mlp.forward(params, mlp.features(family, lo, hi, depth))["z"]
+    assert np.abs(logits - want).max() < 2e-2
+    assert (axis == np.argmax(logits[:, 4:4 + dims], axis=1)).all()
+
+
+def test_tcgen05_wait_timeout_returns_error(cp, oracle, prover):
+    """A completion wait of the tcgen05 kernel that runs out (limit 0: no poll)
+    makes the kernel drain the MMA in flight, free its tensor memory and raise
+    its error flag; the call returns CP_ERR_DEVICE and the handle keeps working
+    once the time-out is cleared."""
+    family = cp.MIDDLE
+    params = mlp.init_params(51)
+    prover.model_set_params(family, params)
+    idx = boxgen.lattice_indices(family, [64, 16, 16, 8], 2000, 27)
+    lo, hi = oracle.lattice_boxes(family, boxgen.LAMBDA, [64, 16, 16, 8], idx)
+    try:
+        prover.model_set_inference(1)
+        good, _, _ = prover.model_predict(family, lo, hi)
+        prover.model_set_wait_limit(0)
+        with pytest.raises(cp.ProverError) as e:
+            prover.model_predict(family, lo, hi)
+        assert e.value.status == 5  # CP_ERR_DEVICE
+        prover.model_set_wait_limit(1 << 22)
+        prover.model_set_inference(1)  # clears the recorded time-out
+        again, _, _ = prover.model_predict(family, lo, hi)
+    finally:
+        prover.model_set_wait_limit(1 << 22)
+        prover.model_set_inference(0)
+    assert (again == good).all()

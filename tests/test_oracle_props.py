@@ -82,3 +82,29 @@ def test_reference_loop_small(oracle):
     steps, proved = oracle.reference_loop(3, [16, 4, 4, 2], max_steps=40)
     assert len(steps) > 0
     assert (steps[:, 0] <= steps[:, 1]).all()
+
+
+@pytest.mark.parametrize("family", range(6))
+def test_decide_path_op_counts(oracle, family):
+    """The reference kernel's own path (stop at the first failing sub-check and
+    handle) costs no more than evaluating every sub-criterion, and exactly as
+    much on proved boxes, where nothing stops early."""
+    dims = boxgen.DIMS[family]
+    sizes = [64, 16, 16, 8][:dims]
+    idx = boxgen.lattice_indices(family, sizes, 2000, seed=10 + family)
+    lo, hi = oracle.lattice_boxes(family, boxgen.LAMBDA, sizes, idx)
+    v, _ = oracle.eval_boxes(family, lo, hi)
+    full = oracle.count_ops(family, lo, hi)
+    dec = oracle.count_ops(family, lo, hi, decide=True)
+    for k in ("add", "mul", "div", "asin"):
+        assert dec[k] <= full[k]
+    proved = v == 0
+    if proved.any():
+        pf = oracle.count_ops(family, lo[:, proved], hi[:, proved])
+        pd = oracle.count_ops(family, lo[:, proved], hi[:, proved], decide=True)
+        assert pf == pd
+    crit = v == 1
+    if crit.any() and family in (0, 3, 4, 5):
+        cf = oracle.count_ops(family, lo[:, crit], hi[:, crit])
+        cd = oracle.count_ops(family, lo[:, crit], hi[:, crit], decide=True)
+        assert cd["asin"] < cf["asin"]

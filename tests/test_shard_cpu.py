@@ -24,7 +24,7 @@ def _worker(rank, world, port, out):
     lo, hi = cp.lambda_shard(rank, world)
     rep = {"evaluated": 10 + rank, "unresolved": rank, "clipped": 0, "fp32_decided": 0, "handles_evaluated": 3,
            "verdicts": [1, 2 + rank, 0, 0, 0], "device_ms": 1.0 + rank, "wall_ms": 2.0 * (1 + rank),
-           "per_depth": [1]}
+           "launches": 2 + rank, "per_depth": [4, 5 + rank] + [1] * rank, "max_depth_seen": 1 + rank}
     tot = cp.reduce_report(rep)
     out[rank] = (lo, hi, tot)
     dist.destroy_process_group()
@@ -53,3 +53,5 @@ def test_two_rank_reduction_gloo():
     for t in (t0, t1):
         assert t["evaluated"] == 21 and t["unresolved"] == 1 and t["verdicts"][1] == 5
         assert t["device_ms"] == 2.0 and t["wall_ms"] == 4.0
+        # per-depth histograms are summed bin by bin; the deepest bin of any rank counts
+        assert t["per_depth"] == [8, 11, 1] and t["max_depth_seen"] == 2 and t["launches"] == 5
