@@ -42,7 +42,8 @@ FAMILIES = range(6)
 DIMS = (4, 3, 4, 4, 3, 4)
 SEED_RES = 64
 LEVEL_CAP = 1 << 25
-SHARD = (0.5, 0.9900000000000001)  # this rank's lambda piece (the whole domain on one GPU)
+SHARD = (0.5, 0.9900000000000001)  # lambda range of the seeds (the whole domain)
+PART, PARTS = 0, 1  # this rank's interleaved piece of every lattice seed (strong scaling over ranks)
 
 
 _T0 = time.perf_counter()
@@ -186,7 +187,7 @@ def seed_opts(family, form, depth, digest=False):
     return dict(precision=form["precision"], policy=cp.SPLIT_UNIFORM, max_depth=depth,
                 seed_sizes=[SEED_RES] * DIMS[family], seed_lambda=SHARD,
                 level_capacity=LEVEL_CAP, engine=form["engine"], learned_order=form.get("learned_order", False),
-                digest=digest)
+                digest=digest, seed_part=PART, seed_parts=PARTS)
 
 
 def run_step(prover, forms, depth, digest=False):
@@ -277,7 +278,7 @@ def proof_leg(prover, cp, forms, families, world=1):
     out = []
     for f in families:
         kw = dict(policy=cp.SPLIT_LAMBDA, max_depth=PROOF_DEPTH, seed_sizes=list(PROOF_SEEDS[f]),
-                  seed_lambda=SHARD, level_capacity=1 << 23)
+                  seed_lambda=SHARD, level_capacity=1 << 23, seed_part=PART, seed_parts=PARTS)
         best_kw = dict(kw, precision=forms[f]["precision"], engine=cp.ENGINE_GRAPH,
                        learned_order=forms[f].get("learned_order", False))
         # the graph engine suits the proof's many small chunks; shape as tuned
@@ -314,7 +315,7 @@ def seed_boxes_host(family):
     import circlepacking_b200 as cp
 
     total = SEED_RES ** DIMS[family]
-    idx = torch.arange(total, device="cuda", dtype=torch.int64)
+    idx = torch.from_numpy(cp.seed_partition(total, PART, PARTS)).cuda()  # this rank's piece of the seed
     lo, hi, vis = cp.lattice_boxes(family, SHARD, [SEED_RES] * DIMS[family], idx, visited=True)
     hlo = torch.empty(lo.shape, dtype=torch.float64, pin_memory=True)
     hhi = torch.empty(hi.shape, dtype=torch.float64, pin_memory=True)
@@ -559,7 +560,7 @@ def main_reference(args, world, rank):
         res.append(cpu_baseline(args.cpu_seconds / max(args.steps, 1)))
     v = float(np.mean([r["value"] for r in res]))
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": "64^dims lattice seed boxes of the six lane-packing families (sampled)",
                        "parallelism": "host threads"},
@@ -570,7 +571,7 @@ def main_reference(args, world, rank):
 
 def main():
     args = parse()
-    global FAMILIES, SEED_RES, LEVEL_CAP, SHARD
+    global FAMILIES, SEED_RES, LEVEL_CAP, PART, PARTS
     FAMILIES = [int(x) for x in args.families.split(",")]
     SEED_RES, LEVEL_CAP = args.seed_res, args.level_capacity
     world, rank, local = dist_init()
@@ -581,9 +582,10 @@ def main():
 
     import circlepacking_b200 as cp
 
-    # lambda sharding: each rank refines its own piece of the domain from a full
-    # 64^dims seed (weak scaling); boxes are independent, so no data exchange
-    SHARD = cp.lambda_shard(rank, world)
+    # strong scaling: every rank refines an interleaved piece of the same seeds
+    # (lattice boxes rank, rank + world, ...); boxes are independent, so the
+    # pieces need no data exchange and their counts and digests add up
+    PART, PARTS = rank, world
 
     torch.cuda.set_device(local)
     prover = cp.Prover(local)
@@ -696,7 +698,7 @@ def main():
         # the same proofs by the reference's own method (run_kernel.cuh:61-132 with
         # the lattice sizes of its family kernels), timed on this GPU
         for f in [int(x) for x in args.reference_proof.split(",")]:
-            if f not in FAMILIES or SHARD != (cp.LAMBDA_MIN, cp.LAMBDA_MAX):
+            if f not in FAMILIES or PARTS != 1:
                 continue
             prover.set_level_variant(f, FP64, 0)
             t0 = time.perf_counter()
@@ -725,7 +727,7 @@ def main():
     roofline = roofline_of(cp, local, reps_best, counts) if counts else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_best, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "ms_per_step": ms_best, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": f"uniform-bisection box set: 64^dims lattice seed per family over lambda [0.5,0.99], "
                                f"not-proved boxes bisected on all axes, {args.depth} levels, six families",
@@ -734,7 +736,8 @@ def main():
                            "when faster (identical verdicts)",
                    "autotune": tuning, "models": models, "boxes_per_step": boxes_step,
                    "l2": "worklists of several GB per level (inputs > L2)",
-                   "parallelism": f"lambda shards x{world} (each rank: 64^dims seed over its lambda piece)"},
+                   "parallelism": f"seed pieces x{world} (rank r refines lattice boxes r, r+{world}, ... of every "
+                                  f"seed; counts and digests summed over ranks)"},
         "plain_fp64": {"value": plain_value, "ms_per_step": ms_plain,
                        "form": "fp64, host-driven level loop, kernel variant 0, reference criterion order"},
         "verdicts_identical": identical,

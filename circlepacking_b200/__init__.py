@@ -194,7 +194,7 @@ class RefineOpts(ctypes.Structure):
                 ("max_depth", ctypes.c_int32), ("seed_sizes", ctypes.c_int32 * 4), ("seed_lambda", ctypes.c_double * 2),
                 ("level_capacity", ctypes.c_int64), ("block", ctypes.c_int32), ("learned_order", ctypes.c_int32),
                 ("engine", ctypes.c_int32), ("boxes_per_thread", ctypes.c_int32), ("lambda_scale", ctypes.c_double),
-                ("digest", ctypes.c_int32)]
+                ("digest", ctypes.c_int32), ("seed_parts", ctypes.c_int32), ("seed_part", ctypes.c_int32)]
 
 
 class RefineReport(ctypes.Structure):
@@ -310,7 +310,7 @@ class Prover:
     @staticmethod
     def opts(family, precision=FP64, policy=SPLIT_UNIFORM, max_depth=2, seed_sizes=None, seed_lambda=None,
              level_capacity=0, learned_order=False, engine=ENGINE_LEVELS, block=0, boxes_per_thread=0,
-             lambda_scale=0.0, digest=False) -> RefineOpts:
+             lambda_scale=0.0, digest=False, seed_part=0, seed_parts=1) -> RefineOpts:
         o = RefineOpts()
         o.family, o.precision, o.policy, o.max_depth = family, precision, policy, max_depth
         ss = list(seed_sizes or [64] * DIMS[family]) + [1] * 4
@@ -325,6 +325,7 @@ class Prover:
         o.boxes_per_thread = boxes_per_thread
         o.lambda_scale = lambda_scale
         o.digest = int(bool(digest))
+        o.seed_parts, o.seed_part = seed_parts, seed_part
         return o
 
     def autotune(self, family, **kw):
@@ -460,6 +461,8 @@ def _declare_model(L):
     L.cp_model_get_params.argtypes = [P, I, P]
     L.cp_model_set_params.argtypes = [P, I, P]
     L.cp_model_loss_grad.argtypes = [I, P, P, P, P, SZ, P, P]
+    L.cp_model_loss_grad_kind.argtypes = [I, I, P, P, P, P, SZ, P, P]
+    L.cp_model_set_training.argtypes = [P, I]
     L.cp_model_predict.argtypes = [P, I, P, P, P, SZ, P, P, P]
     L.cp_model_set_inference.argtypes = [P, I]
     L.cp_model_set_wait_limit.argtypes = [P, ctypes.c_int32]
@@ -469,8 +472,9 @@ def model_param_count() -> int:
     return int(lib().cp_model_param_count())
 
 
-def model_loss_grad(family, params, feats, crit, axis):
-    """One GPU forward+backward pass (no optimiser step): (loss, grad)."""
+def model_loss_grad(family, params, feats, crit, axis, kind=0):
+    """One GPU forward+backward pass (no optimiser step): (loss, grad).
+    kind 0: warp-level mma.sync kernel; 1: tcgen05 kernel (tensor memory)."""
     L = lib()
     _declare_model(L)
     params = np.ascontiguousarray(params, np.float32)
@@ -479,8 +483,9 @@ def model_loss_grad(family, params, feats, crit, axis):
     axis = np.ascontiguousarray(axis, np.int8)
     loss = np.zeros(1, np.float32)
     grad = np.zeros(params.size, np.float32)
-    _check(L.cp_model_loss_grad(family, params.ctypes.data, feats.ctypes.data, crit.ctypes.data, axis.ctypes.data,
-                                feats.shape[0], loss.ctypes.data, grad.ctypes.data), "cp_model_loss_grad")
+    _check(L.cp_model_loss_grad_kind(kind, family, params.ctypes.data, feats.ctypes.data, crit.ctypes.data,
+                                     axis.ctypes.data, feats.shape[0], loss.ctypes.data, grad.ctypes.data),
+           "cp_model_loss_grad")
     return float(loss[0]), grad
 
 
@@ -529,6 +534,11 @@ class _ModelMixin:
         _declare_model(self._L)
         _check(self._L.cp_model_set_inference(self._h, kind), "cp_model_set_inference")
 
+    def model_set_training(self, kind):
+        """The training kernel of model_train: 1 = tcgen05 (default), 0 = mma.sync."""
+        _declare_model(self._L)
+        _check(self._L.cp_model_set_training(self._h, kind), "cp_model_set_training")
+
     def model_set_wait_limit(self, polls):
         """Polls per bounded completion wait of the tcgen05 inference kernel (0: every wait times out)."""
         _declare_model(self._L)
@@ -549,28 +559,50 @@ class _ModelMixin:
 
 
 for _name in ("model_collect", "model_records", "model_train", "model_params", "model_set_params", "model_predict",
-              "model_set_inference", "model_set_wait_limit"):
+              "model_set_inference", "model_set_wait_limit", "model_set_training"):
     setattr(Prover, _name, getattr(_ModelMixin, _name))
 
 
 # ---------------------------------------------------------------- multi-GPU sharding
-def lambda_shard(rank: int, world: int, lo: float = LAMBDA_MIN, hi: float = LAMBDA_MAX):
-    """The lambda sub-range of `rank` among `world` ranks: [lo, hi] cut into
-    `world` equal pieces; neighbouring ranks compute their shared boundary by the
-    same expression, so the pieces tile [lo, hi] exactly (no gap, no overlap
-    beyond the shared endpoint).  Boxes are independent, so ranks refine their
-    pieces with no data exchange; only the final counts are summed."""
+def lambda_shard(rank: int, world: int, lo: float = LAMBDA_MIN, hi: float = LAMBDA_MAX, balance: str = "work"):
+    """The lambda sub-range of `rank` among `world` ranks.
+
+    balance="work": the cut points equalise the integral of (1 - lambda)^-2 over
+    the pieces -- the needed lambda width of the proofs shrinks about like
+    (1 - lambda)^2 toward the top of the domain, so the boxes per unit of lambda
+    grow like its inverse, and equal pieces of that integral carry about equal
+    work.  balance="width": equal widths.  Neighbouring ranks compute their shared
+    boundary by the same expression, so the pieces tile [lo, hi] exactly.  Boxes
+    are independent: ranks refine their pieces with no data exchange and only
+    the final counts are summed (reduce_report)."""
     if world < 1 or not (0 <= rank < world):
         raise ValueError("rank must be in [0, world)")
+    if balance not in ("work", "width"):
+        raise ValueError("balance must be 'work' or 'width'")
 
     def cut(k):
         if k == 0:
             return lo
         if k == world:
             return hi
-        return lo + (hi - lo) / world * k
+        if balance == "width":
+            return lo + (hi - lo) / world * k
+        # W(x) = 1 / (1 - x) is an antiderivative of (1 - x)^-2
+        a, b = 1.0 / (1.0 - lo), 1.0 / (1.0 - hi)
+        return 1.0 - 1.0 / (a + (b - a) * k / world)
 
     return cut(rank), cut(rank + 1)
+
+
+def seed_partition(total: int, rank: int, world: int) -> np.ndarray:
+    """The lattice indices of `rank`'s piece of a seed of `total` boxes split
+    among `world` ranks (cp_refine_opts.seed_part / seed_parts): rank, rank +
+    world, rank + 2 world, ...  Interleaving spreads the lambda slabs, where the
+    work concentrates, evenly over the ranks; the pieces are disjoint and their
+    union is the whole seed, so the ranks' reports add up to the single-GPU one."""
+    if world < 1 or not (0 <= rank < world):
+        raise ValueError("rank must be in [0, world)")
+    return np.arange(rank, total, world, dtype=np.int64)
 
 
 def reduce_report(report: dict, group=None) -> dict:
@@ -578,9 +610,14 @@ def reduce_report(report: dict, group=None) -> dict:
     group (any backend): the scalar counts, the verdict histogram, the launches
     and the per-depth histogram (padded to 64 depths, the report's bins);
     max_depth_seen is recomputed from the summed histogram and the times become
-    the maximum over ranks.  Every rank must call it (two all-reduces)."""
+    the maximum over ranks; a per-box digest is combined as the device combines
+    it (sum mod 2^64, xor), which is exact for disjoint pieces of a seed.  Every
+    rank must call it (two all-reduces, and an all-gather when the report
+    carries a digest)."""
     import torch
     import torch.distributed as dist
+
+    import numpy as _np
 
     keys = ("evaluated", "unresolved", "clipped", "fp32_decided", "handles_evaluated", "launches")
     depth = list(report["per_depth"])[:64]
@@ -602,4 +639,18 @@ def reduce_report(report: dict, group=None) -> dict:
     out["per_depth"] = hist[: seen + 1]
     out["max_depth_seen"] = seen
     out["device_ms"], out["wall_ms"] = t
+    if "digest" in report:
+        # digests add up over disjoint pieces: sum mod 2^64 and xor (gathered:
+        # collectives have no xor for every backend)
+        world = dist.get_world_size(group)
+        mine = torch.tensor([int(x) - (1 << 64) if int(x) >= (1 << 63) else int(x) for x in report["digest"]],
+                            dtype=torch.int64)
+        if dist.get_backend(group) == "nccl":
+            mine = mine.cuda()
+        parts = [torch.zeros_like(mine) for _ in range(world)]
+        dist.all_gather(parts, mine, group=group)
+        words = _np.array([p_.cpu().numpy().view(_np.uint64) for p_ in parts], dtype=_np.uint64)
+        with _np.errstate(over="ignore"):
+            total = int(words[:, 0].sum(dtype=_np.uint64))
+        out["digest"] = (total, int(_np.bitwise_xor.reduce(words[:, 1])))
     return out

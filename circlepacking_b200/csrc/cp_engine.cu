@@ -51,11 +51,14 @@ __global__ void __launch_bounds__(kEvalBlock, MINB) k_level(LevelArgs a) {
 }
 
 // Seed: every box of a family lattice, depth 0.
-__global__ void k_seed(LatticeSpec s, const double* __restrict__ slab_single, size_t total, BoxList out) {
+// Lattice seed: box t of this part is lattice box part + t * parts (the lattice
+// split into `parts` interleaved pieces; parts = 1: the whole lattice in order).
+__global__ void k_seed(LatticeSpec s, const double* __restrict__ slab_single, size_t total, size_t part, size_t parts,
+                       BoxList out) {
     const int D = family_dims(s.fam);
     const size_t step = (size_t)gridDim.x * blockDim.x;
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += step) {
-        size_t rem = t;
+        size_t rem = part + t * parts;
         int ix[4] = {0, 0, 0, 0};
         for (int d = D - 1; d >= 0; --d) {
             ix[d] = (int)(rem % (size_t)s.n[d]);
@@ -723,6 +726,8 @@ cp_status check_opts(const cp_refine_opts* o) {
     if (o->max_depth < 0 || o->max_depth > 250) return CP_ERR_INVALID;
     if (o->engine != CP_ENGINE_LEVELS && o->engine != CP_ENGINE_GRAPH) return CP_ERR_INVALID;
     if (o->boxes_per_thread < 0 || o->boxes_per_thread > 8) return CP_ERR_INVALID;
+    if (o->seed_parts < 0 || (o->seed_parts > 1 && (o->seed_part < 0 || o->seed_part >= o->seed_parts)))
+        return CP_ERR_INVALID;
     return CP_OK;
 }
 
@@ -817,13 +822,19 @@ cp_status cp_refine(cp_prover* p, const cp_refine_opts* o, cp_refine_report* r) 
         s.n[d] = o->seed_sizes[d];
         total *= (size_t)s.n[d];
     }
+    // this call's piece of the lattice: boxes part, part + parts, part + 2 parts, ...
+    const size_t parts = o->seed_parts > 1 ? (size_t)o->seed_parts : 1;
+    const size_t part = parts > 1 ? (size_t)o->seed_part : 0;
+    if (part >= parts) return cp_fail(CP_ERR_INVALID, "cp_refine: seed_part must be in [0, seed_parts)");
+    const size_t lattice_total = total;
+    total = lattice_total > part ? (lattice_total - part + parts - 1) / parts : 0;
     const size_t cap = o->level_capacity > 0 ? (size_t)o->level_capacity : ((size_t)1 << 25);
     if (total > cap) return CP_ERR_CAPACITY;
     CP_TRY(ensure_levels(p, o->max_depth + 1, D, cap));
     for (auto& L : p->levels) L.n = 0;
     CP_TRY(ensure_slab(p, s.n[0]));
     CP_TRY(cp_launch_slab_single(s, p->slab_single, p->stream));
-    k_seed<<<grid_of(k_seed, 128), 128, 0, p->stream>>>(s, p->slab_single, total, p->levels[0].b);
+    k_seed<<<grid_of(k_seed, 128), 128, 0, p->stream>>>(s, p->slab_single, total, part, parts, p->levels[0].b);
     CP_TRY(cp_check_launch());
     p->levels[0].n = total;
     CP_TRY(reset_counters(p));

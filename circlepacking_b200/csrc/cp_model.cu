@@ -845,6 +845,287 @@ __global__ void __launch_bounds__(kTcRows) k_infer_tc(TcArgs ta) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
 }
 
+// ------------------------------------------------------------------ training on tcgen05
+// One fused forward + backward pass of 128 rows per CTA on the 5th-generation
+// tensor cores.  Every product runs as tcgen05.mma (M = 128, BF16 operands in
+// shared memory in the canonical K-major core-matrix layout, FP32 accumulators
+// in tensor memory); each thread owns one row, reads its accumulator row back
+// with tcgen05.ld and writes the next operand tiles:
+//   H1 = X W1,  H2 = G1 W2,  Z = G2 W3                        (forward)
+//   dG2 = dZ W3^T,  dG1 = dH2 W2^T                             (data gradients)
+//   dW2 = G1^T dH2,  dW3 = G2^T dZ,  dW1^T = dH1^T X          (weight gradients, K = the 128 rows)
+// The weight-gradient products have 64 real output rows; their A tiles are
+// 128 rows high with rows 64..127 zero, so every product uses the M = 128
+// accumulator layout (row r in tensor-memory lane r).  Gradients of the CTA's
+// rows are added to a.grad with FP32 atomics.  Completion waits are bounded: on
+// a time-out the kernel raises *err, drains the MMAs in flight, frees its
+// tensor memory and returns.
+constexpr uint32_t kTtCols = 512;
+// accumulator columns (each product's block starts on a multiple of 64 columns)
+constexpr uint32_t TT_H1 = 0, TT_H2 = 64, TT_Z = 128, TT_DG2 = 192, TT_DG1 = 256, TT_DW2 = 320, TT_DW3 = 384,
+                   TT_DW1 = 448;
+
+struct TtSmem {
+    bf16 x[kTcRows * NK];      // A of H1 (K = 16 inputs)
+    bf16 xt[NK * kTcRows];     // B of dW1^T (N = 16 inputs, K = 128 rows)
+    bf16 g1[kTcRows * NH];     // A of H2
+    bf16 g1t[kTcRows * kTcRows];  // A of dW2 (64 hidden units + 64 zero rows, K = 128 rows)
+    bf16 g2[kTcRows * NH];     // A of Z
+    bf16 g2t[kTcRows * kTcRows];  // A of dW3
+    bf16 dz[kTcRows * 16];     // A of dG2 (K = 16: 8 logits, 8 zero)
+    bf16 dzt[16 * kTcRows];    // B of dW3 (N = 16, K = 128 rows)
+    bf16 dh2[kTcRows * NH];    // A of dG1
+    bf16 dh2t[NH * kTcRows];   // B of dW2 (N = 64, K = 128 rows)
+    bf16 dh1t[kTcRows * kTcRows];  // A of dW1^T
+    bf16 w1t[NH * NK];         // B of H1: W1^T (N = 64, K = 16)
+    bf16 w2t[NH * NH];         // B of H2: W2^T
+    bf16 w3t[16 * NH];         // B of Z: W3^T padded to N = 16
+    bf16 w3[NH * 16];          // B of dG2: W3 (N = 64, K = 16: 8 logits, 8 zero)
+    bf16 w2[NH * NH];          // B of dG1: W2 (N = 64, K = 64)
+    float b1[NH], b2[NH], b3[16];
+    float colsum[NH + NH + 16];  // bias gradients of the CTA's rows: db1, db2, db3
+    float loss;
+    unsigned long long mbar;
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t* r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// D (tensor memory, column dcol) = A (128 x K tile) * B (N x K tile)^T, K = 16 * ksteps
+__device__ __forceinline__ void tt_gemm(uint32_t tmem, uint32_t dcol, const bf16* A, const bf16* B, int K, int N) {
+    const uint32_t a = smem_u32(A), b = smem_u32(B), sbo = (uint32_t)K * 16u;
+    for (int ks = 0; ks < K / 16; ++ks)
+        tc_mma(tmem + dcol, sdesc(a + 256u * ks, 128, sbo), sdesc(b + 256u * ks, 128, sbo), tc_idesc(N), ks > 0 ? 1u : 0u);
+}
+
+struct TtArgs {
+    TrainArgs t;
+    int* err;
+    int wait_limit;
+};
+
+__global__ void __launch_bounds__(kTcRows) k_train_tc(TtArgs ta) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TtSmem& s = *reinterpret_cast<TtSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const TrainArgs& a = ta.t;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (blockIdx.x == 0 && tid == 0 && a.step) atomicAdd(a.step, 1);
+    // weights (BF16 views), biases, zero pads
+    for (int i = tid; i < NH * NK; i += kTcRows) s.w1t[cm_off(i / NK, i % NK, NK)] = a.views[V_W1T + i];
+    for (int i = tid; i < NH * NH; i += kTcRows) {
+        s.w2t[cm_off(i / NH, i % NH, NH)] = a.views[V_W2T + i];
+        s.w2[cm_off(i / NH, i % NH, NH)] = a.views[V_W2 + i];
+    }
+    for (int i = tid; i < 16 * NH; i += kTcRows) {
+        const int n = i / NH, k = i % NH;
+        s.w3t[cm_off(n, k, NH)] = n < NO ? a.views[V_W3T + n * NH + k] : __float2bfloat16(0.f);
+        const int i2 = i / 16, o = i % 16;  // W3 as [64 hidden][16 logits, zero padded]
+        s.w3[cm_off(i2, o, 16)] = o < NO ? a.views[V_W3 + i2 * NO + o] : __float2bfloat16(0.f);
+    }
+    for (int i = tid; i < NH; i += kTcRows) {
+        s.b1[i] = a.master[P_B1 + i];
+        s.b2[i] = a.master[P_B2 + i];
+    }
+    if (tid < 16) s.b3[tid] = tid < NO ? a.master[P_B3 + tid] : 0.f;
+    for (int i = tid; i < NH + NH + 16; i += kTcRows) s.colsum[i] = 0.f;
+    if (tid == 0) s.loss = 0.f;
+    // rows 64..127 of the weight-gradient A tiles stay zero
+    for (int i = tid; i < (kTcRows - NH) * kTcRows; i += kTcRows) {
+        const int r = NH + i / kTcRows, k = i % kTcRows;
+        s.g1t[cm_off(r, k, kTcRows)] = __float2bfloat16(0.f);
+        s.g2t[cm_off(r, k, kTcRows)] = __float2bfloat16(0.f);
+        s.dh1t[cm_off(r, k, kTcRows)] = __float2bfloat16(0.f);
+    }
+    // this thread's row: features
+    const size_t row = a.row0 + (size_t)blockIdx.x * kTcRows + tid;
+    const bool valid = row < a.row0 + a.rows && row < a.n;
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+        const bf16 v = valid ? a.feats[row * NK + k] : __float2bfloat16(0.f);
+        s.x[cm_off(tid, k, NK)] = v;
+        s.xt[cm_off(k, tid, kTcRows)] = v;
+    }
+    const uint32_t mbar = smem_u32(&s.mbar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem)),
+                     "r"(kTtCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    uint32_t phase = 0;
+    bool ok = true;
+    uint32_t tmem = 0;
+    // one stage: make the operand tiles visible to the tensor cores, issue, wait
+    auto stage = [&](int which) -> bool {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        tmem = s.tmem;
+        if (tid == 0) {
+            switch (which) {
+            case 0: tt_gemm(tmem, TT_H1, s.x, s.w1t, NK, NH); break;
+            case 1: tt_gemm(tmem, TT_H2, s.g1, s.w2t, NH, NH); break;
+            case 2: tt_gemm(tmem, TT_Z, s.g2, s.w3t, NH, 16); break;
+            case 3: tt_gemm(tmem, TT_DG2, s.dz, s.w3, 16, NH); break;
+            case 4:
+                tt_gemm(tmem, TT_DG1, s.dh2, s.w2, NH, NH);
+                tt_gemm(tmem, TT_DW2, s.g1t, s.dh2t, kTcRows, NH);
+                tt_gemm(tmem, TT_DW3, s.g2t, s.dzt, kTcRows, 16);
+                break;
+            default: tt_gemm(tmem, TT_DW1, s.dh1t, s.xt, kTcRows, 16); break;
+            }
+            tc_commit(mbar);
+        }
+        const bool done = __syncthreads_and(mbar_wait(mbar, phase, ta.wait_limit) ? 1 : 0) != 0;  // block-uniform
+        if (done) phase ^= 1u;  // after a time-out `phase` names the pending phase (drained below)
+        tc_fence_after();
+        return done;
+    };
+    uint32_t r[32], q[32];
+    do {
+        // ---- forward
+        if (!(ok = stage(0))) break;
+        for (int c0 = 0; c0 < NH; c0 += 32) {
+            tc_ld32(tmem + lane_base + TT_H1 + c0, r);
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                const bf16 g = __float2bfloat16_rn(gelu(__uint_as_float(r[c]) + s.b1[c0 + c]));
+                s.g1[cm_off(tid, c0 + c, NH)] = g;
+                s.g1t[cm_off(c0 + c, tid, kTcRows)] = g;
+            }
+        }
+        if (!(ok = stage(1))) break;
+        for (int c0 = 0; c0 < NH; c0 += 32) {
+            tc_ld32(tmem + lane_base + TT_H2 + c0, r);
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                const bf16 g = __float2bfloat16_rn(gelu(__uint_as_float(r[c]) + s.b2[c0 + c]));
+                s.g2[cm_off(tid, c0 + c, NH)] = g;
+                s.g2t[cm_off(c0 + c, tid, kTcRows)] = g;
+            }
+        }
+        if (!(ok = stage(2))) break;
+        // ---- loss and dZ of this thread's row
+        {
+            uint32_t zr[16];
+            tc_ld16(tmem + lane_base + TT_Z, zr);
+            float z[NO], dz[NO];
+#pragma unroll
+            for (int k = 0; k < NO; ++k) {
+                z[k] = __uint_as_float(zr[k]) + s.b3[k];
+                dz[k] = 0.f;
+            }
+            float l = 0.f;
+            if (valid) {
+                const unsigned bits = a.crit[row];
+                for (int k = 0; k < a.K; ++k) {
+                    const float y = (float)((bits >> k) & 1u);
+                    l += fmaxf(z[k], 0.f) + log1pf(expf(-fabsf(z[k]))) - y * z[k];
+                    dz[k] = (1.f / (1.f + expf(-z[k])) - y) * a.inv_batch;
+                }
+                const int lab = a.axis[row];
+                if (lab >= 0) {
+                    float m = -INFINITY;
+                    for (int d = 0; d < a.D; ++d) m = fmaxf(m, z[4 + d]);
+                    float ssum = 0.f;
+                    for (int d = 0; d < a.D; ++d) ssum += expf(z[4 + d] - m);
+                    l += m + logf(ssum) - z[4 + lab];
+                    for (int d = 0; d < a.D; ++d)
+                        dz[4 + d] = (expf(z[4 + d] - m) / ssum - (d == lab ? 1.f : 0.f)) * a.inv_batch;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const float v = k < NO ? dz[k] : 0.f;
+                const bf16 b = __float2bfloat16_rn(v);
+                s.dz[cm_off(tid, k, 16)] = b;
+                s.dzt[cm_off(k, tid, kTcRows)] = b;
+                if (k < NO && v != 0.f) atomicAdd(&s.colsum[NH + NH + k], v);
+            }
+            for (int off = 16; off > 0; off >>= 1) l += __shfl_xor_sync(0xffffffffu, l, off);
+            if (lane == 0 && l != 0.f) atomicAdd(&s.loss, l);
+        }
+        // ---- dH2 = (dZ W3^T) * gelu'(H2)
+        if (!(ok = stage(3))) break;
+        for (int c0 = 0; c0 < NH; c0 += 32) {
+            tc_ld32(tmem + lane_base + TT_DG2 + c0, r);
+            tc_ld32(tmem + lane_base + TT_H2 + c0, q);
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                const float d = __uint_as_float(r[c]) * gelu_grad(__uint_as_float(q[c]) + s.b2[c0 + c]);
+                const bf16 b = __float2bfloat16_rn(d);
+                s.dh2[cm_off(tid, c0 + c, NH)] = b;
+                s.dh2t[cm_off(c0 + c, tid, kTcRows)] = b;
+                if (d != 0.f) atomicAdd(&s.colsum[NH + c0 + c], d);
+            }
+        }
+        // ---- dH1 = (dH2 W2^T) * gelu'(H1); dW2 and dW3 in the same stage
+        if (!(ok = stage(4))) break;
+        for (int c0 = 0; c0 < NH; c0 += 32) {
+            tc_ld32(tmem + lane_base + TT_DG1 + c0, r);
+            tc_ld32(tmem + lane_base + TT_H1 + c0, q);
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                const float d = __uint_as_float(r[c]) * gelu_grad(__uint_as_float(q[c]) + s.b1[c0 + c]);
+                s.dh1t[cm_off(c0 + c, tid, kTcRows)] = __float2bfloat16_rn(d);
+                if (d != 0.f) atomicAdd(&s.colsum[c0 + c], d);
+            }
+        }
+        // dW2 (rows = hidden units 0..63 in lanes 0..63: warps 0 and 1)
+        if (warp < 2) {
+            for (int c0 = 0; c0 < NH; c0 += 32) {
+                tc_ld32(tmem + lane_base + TT_DW2 + c0, r);
+#pragma unroll
+                for (int c = 0; c < 32; ++c) atomicAdd(&a.grad[P_W2 + tid * NH + c0 + c], __uint_as_float(r[c]));
+            }
+            uint32_t w3r[16];
+            tc_ld16(tmem + lane_base + TT_DW3, w3r);
+#pragma unroll
+            for (int o = 0; o < NO; ++o) atomicAdd(&a.grad[P_W3 + tid * NO + o], __uint_as_float(w3r[o]));
+        }
+        if (!(ok = stage(5))) break;
+        if (warp < 2) {
+            uint32_t w1r[16];
+            tc_ld16(tmem + lane_base + TT_DW1, w1r);  // dW1^T row = hidden unit tid, columns = inputs
+#pragma unroll
+            for (int k = 0; k < NK; ++k) atomicAdd(&a.grad[P_W1 + k * NH + tid], __uint_as_float(w1r[k]));
+        }
+    } while (0);
+    if (!ok) {
+        if (tid == 0) atomicExch(ta.err, 1);
+        mbar_wait(mbar, phase);  // bounded: the MMAs committed to the pending phase finish first
+    } else {
+        __syncthreads();
+        for (int i = tid; i < NH + NH + 16; i += kTcRows) {
+            const float v = s.colsum[i];
+            if (v == 0.f) continue;
+            if (i < NH)
+                atomicAdd(&a.grad[P_B1 + i], v);
+            else if (i < 2 * NH)
+                atomicAdd(&a.grad[P_B2 + i - NH], v);
+            else if (i - 2 * NH < NO)
+                atomicAdd(&a.grad[P_B3 + i - 2 * NH], v);
+        }
+        if (tid == 0 && a.loss && s.loss != 0.f) atomicAdd(a.loss, s.loss * a.inv_batch);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s.tmem), "r"(kTtCols) : "memory");
+}
+
 // ------------------------------------------------------------------ trace records
 struct LabelArgs {
     BoxList in;
@@ -971,6 +1252,8 @@ struct ModelState {
     int* tc_err = nullptr;    // device flag raised by a timed-out tcgen05 wait
     int* tc_err_h = nullptr;  // pinned copy, refreshed after every tcgen05 launch
     int tc_wait_limit = kTcWaitLimit;
+    // training kernel: 0 = warp-level mma.sync, 1 = tcgen05 (default)
+    int train_kind = 1;
     // per-chunk hints
     uint8_t* hint_axis = nullptr;
     uint8_t* hint_order = nullptr;
@@ -1045,12 +1328,20 @@ std::vector<float> init_params(uint64_t seed) {
 }
 
 size_t train_smem() { return sizeof(TrainSmem); }
+size_t train_tc_smem() { return sizeof(TtSmem) + 1024; }  // + alignment of the tile base to 1024 B
 
+// Training kernels: 0 = warp-level mma.sync (64 rows per block), 1 = tcgen05
+// with tensor-memory accumulators (128 rows per CTA).  `err` (kind 1): device
+// flag raised by a timed-out completion wait.
 cp_status launch_train(const FamilyModel& f, const bf16* feats, const uint8_t* crit, const int8_t* axis, size_t n,
-                       size_t row0, size_t rows, int fam, cudaStream_t st, bool with_step) {
+                       size_t row0, size_t rows, int fam, cudaStream_t st, bool with_step, int kind = 0,
+                       int* err = nullptr, int wait_limit = kTcWaitLimit) {
     // per-device function attribute: set on every call (cheap), so a handle on
     // another device gets it too
-    cudaError_t e = cudaFuncSetAttribute(k_train_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem());
+    cudaError_t e = kind ? cudaFuncSetAttribute(k_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)train_tc_smem())
+                         : cudaFuncSetAttribute(k_train_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)train_smem());
     if (e != cudaSuccess) return cp_record_cuda_error(e, CP_ERR_CUDA);
     TrainArgs a;
     a.feats = feats;
@@ -1067,6 +1358,13 @@ cp_status launch_train(const FamilyModel& f, const bf16* feats, const uint8_t* c
     a.grad = f.grad;
     a.loss = f.loss;
     a.step = with_step ? f.step : nullptr;
+    if (kind) {
+        if (!err) return cp_fail(CP_ERR_INVALID, "tcgen05 training needs an error flag");
+        TtArgs t{a, err, wait_limit};
+        const unsigned grid = (unsigned)((rows + kTcRows - 1) / kTcRows);
+        k_train_tc<<<grid, kTcRows, train_tc_smem(), st>>>(t);
+        return cp_check_launch();
+    }
     const unsigned grid = (unsigned)((rows + kTrainRows - 1) / kTrainRows);
     k_train_step<<<grid, kTrainWarps * 32, train_smem(), st>>>(a);
     return cp_check_launch();
@@ -1350,6 +1648,14 @@ cp_status cp_model_train(cp_prover* p, int family, int epochs, int batch, float 
     FamilyModel& f = m->fam[family];
     M_TRY(ensure_family(f));
     cudaStream_t st = cp_prover_stream(p);
+    if (m->train_kind && !m->tc_err) {
+        M_TRY(ok_or(cudaMalloc(&m->tc_err, sizeof(int))));
+        M_TRY(ok_or(cudaMallocHost(&m->tc_err_h, sizeof(int))));
+        *m->tc_err_h = 0;
+        M_TRY(ok_or(cudaMemsetAsync(m->tc_err, 0, sizeof(int), st)));
+    }
+    if (m->train_kind && *m->tc_err_h)
+        return cp_fail(CP_ERR_DEVICE, "tcgen05 kernels: a tensor-core completion wait timed out earlier");
     const std::vector<float> init = init_params(seed);
     M_TRY(ok_or(cudaMemcpyAsync(f.master, init.data(), sizeof(float) * NPARAM, cudaMemcpyHostToDevice, st)));
     M_TRY(ok_or(cudaMemsetAsync(f.m, 0, sizeof(float) * NPARAM * 3, st)));
@@ -1381,7 +1687,8 @@ cp_status cp_model_train(cp_prover* p, int family, int epochs, int batch, float 
             for (size_t b = 0; b < steps && s == CP_OK; ++b) {
                 const size_t row0 = b * (size_t)batch;
                 const size_t rows = std::min<size_t>((size_t)batch, n - row0);
-                s = launch_train(f, sx, sc, sa, n, row0, rows, family, st, true);
+                s = launch_train(f, sx, sc, sa, n, row0, rows, family, st, true, m->train_kind, m->tc_err,
+                                 m->tc_wait_limit);
                 if (s == CP_OK) {
                     k_adam<<<(NPARAM + 255) / 256, 256, 0, st>>>(f.master, f.m, f.v, f.grad, f.views, f.step, lr);
                     s = cp_check_launch();
@@ -1395,11 +1702,22 @@ cp_status cp_model_train(cp_prover* p, int family, int epochs, int batch, float 
             }
         }
         if (s == CP_OK) s = ok_or(cudaStreamSynchronize(st));
+        if (s == CP_OK && m->train_kind) {
+            s = ok_or(cudaMemcpy(m->tc_err_h, m->tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+            if (s == CP_OK && *m->tc_err_h)
+                s = cp_fail(CP_ERR_DEVICE, "tcgen05 training: a tensor-core completion wait timed out");
+        }
     }
     cudaFree(dperm);
     cudaFree(sx);
     if (s == CP_OK) f.ready = true;
     return s;
+}
+
+cp_status cp_model_set_training(cp_prover* p, int kind) {
+    if (!p || kind < 0 || kind > 1) return cp_fail(CP_ERR_INVALID, "cp_model_set_training: kind 0 or 1");
+    state(p, true)->train_kind = kind;
+    return CP_OK;
 }
 
 cp_status cp_model_get_params(cp_prover* p, int family, float* params) {
@@ -1432,7 +1750,13 @@ int cp_model_param_count(void) { return NPARAM; }
 // for gradient checks.  feats: [n][16] FP32 (rounded to BF16 on the device).
 cp_status cp_model_loss_grad(int family, const float* params, const float* feats, const uint8_t* crit,
                              const int8_t* axis, size_t n, float* loss, float* grad) {
-    if (family < 0 || family > 5 || !params || !feats || !crit || !axis || n == 0 || !loss || !grad)
+    return cp_model_loss_grad_kind(0, family, params, feats, crit, axis, n, loss, grad);
+}
+
+cp_status cp_model_loss_grad_kind(int kind, int family, const float* params, const float* feats, const uint8_t* crit,
+                                  const int8_t* axis, size_t n, float* loss, float* grad) {
+    if (kind < 0 || kind > 1 || family < 0 || family > 5 || !params || !feats || !crit || !axis || n == 0 || !loss ||
+        !grad)
         return cp_fail(CP_ERR_INVALID, "cp_model_loss_grad: bad arguments");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -1442,7 +1766,10 @@ cp_status cp_model_loss_grad(int family, const float* params, const float* feats
     FamilyModel f;
     cp_status s = ensure_family(f);
     bf16* dx = nullptr;
+    int* derr = nullptr;
     if (s == CP_OK) s = ok_or(cudaMalloc(&dx, sizeof(bf16) * NK * n + 2 * n));
+    if (s == CP_OK) s = ok_or(cudaMalloc(&derr, sizeof(int)));
+    if (s == CP_OK) s = ok_or(cudaMemset(derr, 0, sizeof(int)));
     if (s == CP_OK) {
         std::vector<bf16> hx(NK * n);
         for (size_t i = 0; i < NK * n; ++i) hx[i] = __float2bfloat16_rn(feats[i]);
@@ -1458,12 +1785,16 @@ cp_status cp_model_loss_grad(int family, const float* params, const float* feats
             k_views<<<(NPARAM + 255) / 256, 256>>>(f.master, f.views);
             s = cp_check_launch();
         }
-        if (s == CP_OK) s = launch_train(f, dx, dc, da, n, 0, n, family, 0, false);
+        if (s == CP_OK) s = launch_train(f, dx, dc, da, n, 0, n, family, 0, false, kind, derr);
         if (s == CP_OK) s = ok_or(cudaDeviceSynchronize());
+        int herr = 0;
+        if (s == CP_OK) s = ok_or(cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost));
+        if (s == CP_OK && herr) s = cp_fail(CP_ERR_DEVICE, "tcgen05 training: a tensor-core completion wait timed out");
         if (s == CP_OK) s = ok_or(cudaMemcpy(grad, f.grad, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost));
         if (s == CP_OK) s = ok_or(cudaMemcpy(loss, f.loss, sizeof(float), cudaMemcpyDeviceToHost));
     }
     cudaFree(dx);
+    cudaFree(derr);
     free_family(f);
     return s;
 }

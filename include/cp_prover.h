@@ -191,6 +191,10 @@ typedef struct cp_refine_opts {
     int32_t boxes_per_thread; /* graph engine: boxes a warp lane takes per claim (1..8); 0 = tuned */
     double lambda_scale;    /* CP_SPLIT_HYBRID: lambda target width scale; 0 = 4e-3 */
     int32_t digest;         /* 1 = compute report->digest (per-box verdict identity checks) */
+    int32_t seed_parts;     /* cp_refine: > 1 splits the lattice seed into interleaved pieces ... */
+    int32_t seed_part;      /* ... and refines piece seed_part only: lattice boxes seed_part + k * seed_parts
+                               (one rank's share of the same proof; the pieces' reports add up to the
+                               whole seed's, digests included) */
 } cp_refine_opts;
 
 /* Refinement engines.  CP_ENGINE_LEVELS: the host picks each chunk, launches
@@ -383,6 +387,16 @@ cp_status cp_model_set_params(cp_prover* p, int family, const float* params);
  * gradient checks).  feats [n][16] FP32 (rounded to BF16 on the device). */
 cp_status cp_model_loss_grad(int family, const float* params, const float* feats, const uint8_t* crit,
                              const int8_t* axis, size_t n, float* loss, float* grad);
+
+/* As cp_model_loss_grad on a chosen training kernel: kind 0 = warp-level BF16
+ * mma.sync (64 rows per block), 1 = tcgen05.mma with FP32 accumulators in
+ * tensor memory (128 rows per CTA; bounded completion waits, a time-out
+ * returns CP_ERR_DEVICE). */
+cp_status cp_model_loss_grad_kind(int kind, int family, const float* params, const float* feats, const uint8_t* crit,
+                                  const int8_t* axis, size_t n, float* loss, float* grad);
+
+/* The kernel cp_model_train runs: 1 = tcgen05 (default), 0 = mma.sync. */
+cp_status cp_model_set_training(cp_prover* p, int kind);
 
 /* The kernel that runs the network for hints and predictions: 0 = warp-level
  * BF16 mma.sync (default; also the one used inside the graph engine),

@@ -11,26 +11,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-M64 = (1 << 64) - 1
-
-
-def _mix64(z):
-    z = np.asarray(z, dtype=np.uint64)
-    with np.errstate(over="ignore"):
-        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
-        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
-    return z ^ (z >> np.uint64(31))
-
-
-def host_digest(lo, hi, verdict):
-    """The device's digest of boxes lo/hi (dims, n) with the given verdicts."""
-    with np.errstate(over="ignore"):
-        h = np.uint64(0x9E3779B97F4A7C15) * (verdict.astype(np.uint64) + np.uint64(1))
-        for d in range(lo.shape[0]):
-            h = _mix64(h ^ np.ascontiguousarray(lo[d]).view(np.uint64))
-            h = _mix64(h + np.ascontiguousarray(hi[d]).view(np.uint64))
-        x = _mix64(h ^ np.uint64(0x5851F42D4C957F2D))
-    return int(h.sum(dtype=np.uint64)) & M64, int(np.bitwise_xor.reduce(x)) if x.size else 0
+from tests.boxgen import M64, host_digest
 
 
 @pytest.fixture(scope="module")

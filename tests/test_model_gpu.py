@@ -27,12 +27,16 @@ def _rows(seed, n):
     return x, crit, axis
 
 
+@pytest.mark.parametrize("kind", [0, 1], ids=["mma_sync", "tcgen05"])
 @pytest.mark.parametrize("family,n", [(3, 200), (5, 64), (4, 1000), (0, 130)])
-def test_gradient_matches_oracle(cp, family, n):
+def test_gradient_matches_oracle(cp, family, n, kind):
+    """Loss and gradient of one forward + backward pass on the GPU against the
+    CPU restatement, for both training kernels (warp-level mma.sync and tcgen05
+    with tensor-memory accumulators)."""
     p = mlp.init_params(11 + family)
     x, crit, axis = _rows(family, n)
     axis = np.where(axis >= boxgen.DIMS[family], -1, axis).astype(np.int8)
-    loss, grad = cp.model_loss_grad(family, p, x, crit, axis)
+    loss, grad = cp.model_loss_grad(family, p, x, crit, axis, kind=kind)
     want_loss, want_grad = mlp.loss_grad(family, p, x, crit, axis)
     assert abs(loss - want_loss) <= 1e-4 * abs(want_loss) + 1e-6
     # BF16 operands: the GPU (FP32 accumulation) and the oracle (FP64) may round an
@@ -96,6 +100,7 @@ def test_training_gains_over_plain_order(cp, prover):
     kw = dict(policy=cp.SPLIT_WIDEST, max_depth=8, seed_sizes=[16, 8, 8, 4])
     n = prover.model_collect(family, 400000, sample_stride=2, **kw)
     assert n > 50000
+    prover.model_set_training(1)  # tcgen05 training kernel (the default)
     losses = prover.model_train(family, epochs=8, batch=4096, lr=2e-3, seed=3)
     assert np.isfinite(losses).all() and losses[-1] < 0.8 * losses[0], losses
     plain = prover.refine(family, **kw)
@@ -189,3 +194,20 @@ def test_tcgen05_wait_timeout_returns_error(cp, oracle, prover):
         prover.model_set_wait_limit(1 << 22)
         prover.model_set_inference(0)
     assert (again == good).all()
+
+
+def test_tcgen05_and_mma_sync_training_agree(cp, prover):
+    """Both training kernels reach about the same loss from the same records,
+    initialisation and shuffle (BF16 products summed in another order)."""
+    family = cp.END_3D
+    prover.model_collect(family, 100000, sample_stride=2, policy=cp.SPLIT_WIDEST, max_depth=6,
+                         seed_sizes=[16, 8, 8, 4])
+    try:
+        prover.model_set_training(0)
+        l0 = prover.model_train(family, epochs=4, batch=4096, lr=2e-3, seed=5)
+        prover.model_set_training(1)
+        l1 = prover.model_train(family, epochs=4, batch=4096, lr=2e-3, seed=5)
+    finally:
+        prover.model_set_training(1)
+    assert np.isfinite(l1).all() and l1[-1] < l1[0]
+    assert abs(l1[-1] - l0[-1]) <= 0.05 * abs(l0[-1]) + 1e-3, (l0, l1)
