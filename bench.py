@@ -326,44 +326,6 @@ def seed_boxes_host(family):
     return hlo, hhi, hdp
 
 
-def sample_evaluated_boxes(prover, cp, depth):
-    """A sample of the boxes the step evaluates, per family and depth: every
-    16th box of every chunk of the same uniform refinement from a 16^dims seed
-    down to `depth` levels, recorded by the device (outside the timed region)."""
-    out = {}
-    rng = np.random.default_rng(5)
-    for f in FAMILIES:
-        prover.model_collect(f, 1_500_000, sample_stride=16, policy=cp.SPLIT_UNIFORM, max_depth=depth,
-                             seed_sizes=[16] * DIMS[f], seed_lambda=SHARD, level_capacity=LEVEL_CAP)
-        r = prover.model_records()
-        d = DIMS[f]
-        boxes, dep = r["boxes"], r["depth"].astype(np.int64)
-        keep = np.zeros(dep.size, bool)
-        for k in np.unique(dep):  # at most 40k boxes per depth
-            idx = np.flatnonzero(dep == k)
-            keep[rng.choice(idx, size=min(idx.size, 40_000), replace=False)] = True
-        out[f] = (boxes[keep, 0:2 * d:2].T.copy(), boxes[keep, 1:2 * d:2].T.copy(), dep[keep])
-    return out
-
-
-def op_counts(samples):
-    """Primitive operations per evaluated box of the reference kernel's own path
-    (stop at the first failing sub-check and handle), per family and depth,
-    counted by the CPU restatement's op-counting mode on the sampled boxes.
-    Runs inside the CPU-baseline leg (the restatement is the checker here)."""
-    from oracle import oracle as O
-
-    out = {}
-    for f, (lo, hi, dep) in samples.items():
-        per = {}
-        for d in np.unique(dep):
-            sel = dep == d
-            c = O.count_ops(f, lo[:, sel], hi[:, sel], decide=True)
-            per[int(d)] = {k: c[k] / c["boxes"] for k in ("add", "mul", "div", "asin")} | {"boxes": c["boxes"]}
-        out[f] = per
-    return out
-
-
 def roofline_of(cp, device, reps, counts) -> dict:
     """Roofline of the FP64 criterion evaluation (the level kernel): the
     reference kernel's own primitive operations per evaluated box (add/sub,
@@ -414,38 +376,46 @@ def roofline_of(cp, device, reps, counts) -> dict:
             "ops_per_box": {cp.FAMILIES[f]: {str(d): v for d, v in counts[f].items()} for f in FAMILIES}}
 
 
-def cpu_leg(seconds: float, samples):
-    """The CPU-baseline leg: the CPU restatement timed on the host cores, and its
-    op-counting mode on the sampled boxes of the step (for the roofline)."""
-    return cpu_baseline(seconds), (op_counts(samples) if samples else None)
-
-
-def cpu_baseline(seconds: float) -> dict:
-    """The CPU oracle (all host threads) on a bounded sample of the workload:
-    boxes drawn uniformly from the seed lattices of the families, in rounds of
-    growing size until about `seconds` of CPU time have been spent."""
+def cpu_baseline(seconds: float, depth: int):
+    """The CPU restatement (oracle/cpu_oracle.cpp, all host threads) on a bounded
+    sample of the same workload: the uniform refinement below randomly drawn
+    boxes of each family's 64^dims seed lattice down to `depth` levels, every
+    box on the reference kernel's own evaluation path, in rounds of growing size
+    until about `seconds` of CPU time have been spent.  Returns the baseline and
+    the primitive operations per evaluated box, per family and depth (the
+    roofline's work model)."""
     from oracle import oracle as O
 
     threads = os.cpu_count() or 1
     rng = np.random.default_rng(1)
-    total_boxes, t_total, per_family, rounds = 0, 0.0, 4000, 0
+    boxes, t_total, rounds, seeds = 0, 0.0, 0, 16
+    ops = {f: np.zeros((16, 4), np.float64) for f in FAMILIES}
+    per_depth = {f: np.zeros(16, np.float64) for f in FAMILIES}
+    n_seeds = 0
     while t_total < seconds:
         for f in FAMILIES:
-            dims = DIMS[f]
-            total = SEED_RES ** dims
-            idx = np.sort(rng.choice(total, size=min(per_family, total), replace=False))
-            lo, hi = O.lattice_boxes(f, (0.5, 0.9900000000000001), [SEED_RES] * dims, idx)
+            total = SEED_RES ** DIMS[f]
+            idx = np.sort(rng.choice(total, size=min(seeds, total), replace=False))
             t0 = time.perf_counter()
-            O.eval_boxes(f, lo, hi, threads=threads)
+            r = O.refine_sample(f, [SEED_RES] * DIMS[f], idx, depth, outer=SHARD, threads=threads)
             t_total += time.perf_counter() - t0
-            total_boxes += idx.size
+            boxes += r["evaluated"]
+            n_seeds += idx.size
+            ops[f] += r["ops"]
+            per_depth[f] += np.asarray(r["per_depth"], np.float64)
         rounds += 1
         if t_total < seconds / 3:
-            per_family = min(per_family * 4, 4_000_000)
-    return {"value": total_boxes / t_total, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{total_boxes} boxes drawn from the 64^dims seed lattices of the families "
-                      f"({', '.join(str(f) for f in FAMILIES)}) in {rounds} rounds, CPU restatement "
-                      f"(oracle/cpu_oracle.cpp), {threads} threads, {t_total:.1f} s of evaluation"}
+            seeds = min(seeds * 4, 1 << 16)
+    counts = {}
+    for f in FAMILIES:
+        counts[f] = {d: dict(zip(("add", "mul", "div", "asin"), (ops[f][d] / per_depth[f][d]).tolist()),
+                             boxes=int(per_depth[f][d])) for d in range(16) if per_depth[f][d] > 0}
+    base = {"value": boxes / t_total, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n_seeds} seed boxes drawn from the 64^dims lattices of the families "
+                      f"({', '.join(str(f) for f in FAMILIES)}), each refined with the uniform split to depth "
+                      f"{depth} ({boxes} boxes evaluated on the reference kernel's path), CPU restatement "
+                      f"(oracle/cpu_oracle.cpp), {threads} threads, {t_total:.1f} s, {rounds} rounds"}
+    return base, counts
 
 
 def uneven_seeds(prover, cp, family, n_random):
@@ -555,14 +525,16 @@ def main_reference(args, world, rank):
         return
     res = []
     for _ in range(args.warmup):
-        cpu_baseline(min(2.0, args.cpu_seconds))
+        cpu_baseline(min(2.0, args.cpu_seconds), args.depth)
     for _ in range(args.steps):
-        res.append(cpu_baseline(args.cpu_seconds / max(args.steps, 1)))
+        res.append(cpu_baseline(args.cpu_seconds / max(args.steps, 1), args.depth)[0])
     v = float(np.mean([r["value"] for r in res]))
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": "64^dims lattice seed boxes of the six lane-packing families (sampled)",
+            "config": {"workload": f"uniform-bisection box set: 64^dims lattice seed per family over lambda "
+                                   f"[0.5,0.99], not-proved boxes bisected on all axes, {args.depth} levels, six "
+                                   f"families (sampled seeds, CPU)",
                        "parallelism": "host threads"},
             "cpu_baseline": {**res[-1], "value": v},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -722,9 +694,8 @@ def main():
     # step's boxes; then the roofline of the level kernel (best form)
     cpu, counts = None, None
     if rank == 0 and not args.no_cpu:
-        samples = None if args.no_roofline else sample_evaluated_boxes(prover, cp, args.depth)
-        cpu, counts = cpu_leg(args.cpu_seconds, samples)
-    roofline = roofline_of(cp, local, reps_best, counts) if counts else None
+        cpu, counts = cpu_baseline(args.cpu_seconds, args.depth)
+    roofline = roofline_of(cp, local, reps_best, counts) if (counts and not args.no_roofline) else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_best, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",

@@ -68,10 +68,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
         list(ex.map(lambda s: _compile(s, verbose), todo))
     objs = [os.path.join(OBJ_DIR, os.path.basename(s) + ".o") for s in srcs]
     if todo or force or not os.path.exists(LIB):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        # link to a temporary name and rename: a reader of the tree (a process
+        # loading the library, a copy of the tree) sees the old or the new file,
+        # never a partly written one
+        tmp = LIB + ".tmp"
+        cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, LIB)
     return LIB
 
 

@@ -617,11 +617,19 @@ cp_status build_graph(cp_prover* p, const cp_refine_opts& o, int variant, int bp
     do {
         k_sched<<<1, 32, 0, p->stream>>>(p->d_sched, p->cnt, h);
         if ((st = cp_check_launch()) != CP_OK) break;
-        uint8_t *axis = nullptr, *order = nullptr;
-        if (learned_axis || learned_order) {
-            st = cp_model_graph_hints(p, fam, p->d_sched, p->d_levels, p->level_cap, learned_axis ? &axis : nullptr,
-                                      learned_order ? &order : nullptr);
-            if (st != CP_OK) break;
+        // with a learned policy the level kernel runs the network inline (tcgen05)
+        const bool net = learned_axis || learned_order;
+        NetArgs na{};
+        if (net) {
+            const void* views = nullptr;
+            const float* master = nullptr;
+            int limit = 0;
+            if ((st = cp_model_net_params(p, fam, &views, &master, &limit)) != CP_OK) break;
+            na.views = static_cast<const tc::bf16*>(views);
+            na.master = master;
+            na.wait_limit = limit;
+            na.want_order = learned_order ? 1 : 0;
+            na.want_axis = learned_axis ? 1 : 0;
         }
         PersistArgs pa;
         pa.levels = p->d_levels;
@@ -633,16 +641,21 @@ cp_status build_graph(cp_prover* p, const cp_refine_opts& o, int variant, int bp
         pa.lambda_scale = lambda_scale_of(o);
         pa.max_depth = o.max_depth;
         pa.bpt = bpt;
-        pa.axis_hint = axis;
-        pa.order_hint = order;
+        pa.axis_hint = nullptr;
+        pa.order_hint = nullptr;
         pa.digest = o.digest ? 1 : 0;
-        void* kern = prec ? cp_graph_kernel_fp32(fam, variant) : cp_graph_kernel_fp64(fam, variant);
-        const int block = kGraphBlock[variant];
+        void* kern = net ? (prec ? cp_graph_kernel_net_fp32(fam) : cp_graph_kernel_net_fp64(fam))
+                         : (prec ? cp_graph_kernel_fp32(fam, variant) : cp_graph_kernel_fp64(fam, variant));
+        const int block = net ? kNetBlock : kGraphBlock[variant];
         int per_sm = 0, sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+        // each CTA of the inline-network kernel holds tc::kNetCols tensor-memory columns
+        if (net && per_sm > kNetMaxCtasPerSm) per_sm = kNetMaxCtasPerSm;
         void* args[] = {&pa};
-        st = cuda_ok(cudaLaunchKernel(kern, dim3((unsigned)(sms * per_sm)), dim3((unsigned)block), args, 0, p->stream));
+        void* net_args[] = {&pa, &na};
+        st = cuda_ok(cudaLaunchKernel(kern, dim3((unsigned)(sms * per_sm)), dim3((unsigned)block), net ? net_args : args,
+                                      0, p->stream));
     } while (0);
     cudaGraph_t captured = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(p->stream, &captured);
@@ -680,7 +693,6 @@ cp_status refine_graph(cp_prover* p, const cp_refine_opts& o, cp_refine_report* 
     hs.fanout = fanout(o.policy == CP_SPLIT_LEARNED ? SPLIT_GIVEN : o.policy, D);
     CP_TRY(cuda_ok(cudaMemcpyAsync(p->d_levels, hl, sizeof(BoxList) * nlevels, cudaMemcpyHostToDevice, p->stream)));
     CP_TRY(cuda_ok(cudaMemcpyAsync(p->d_sched, &hs, sizeof(DevSched), cudaMemcpyHostToDevice, p->stream)));
-    if (learned_axis || learned_order) CP_TRY(cp_model_reserve_hints(p, p->level_cap));
     double ls = lambda_scale_of(o);
     unsigned long long ls_bits;
     std::memcpy(&ls_bits, &ls, 8);
@@ -690,7 +702,7 @@ cp_status refine_graph(cp_prover* p, const cp_refine_opts& o, cp_refine_report* 
                                         (unsigned long long)(learned_axis | (learned_order << 1) | (o.digest ? 4 : 0)),
                                         (unsigned long long)(uintptr_t)p->levels[0].b.lo, (unsigned long long)p->level_cap,
                                         (unsigned long long)nlevels,
-                                        (unsigned long long)(uintptr_t)cp_model_hint_buffer(p)};
+                                        (unsigned long long)(uintptr_t)p->model};
     if (!p->graph_exec || std::memcmp(key, p->graph_key, sizeof(key)) != 0) {
         CP_TRY(build_graph(p, o, variant, bpt, learned_axis, learned_order));
         std::memcpy(p->graph_key, key, sizeof(key));
@@ -704,6 +716,8 @@ cp_status refine_graph(cp_prover* p, const cp_refine_opts& o, cp_refine_report* 
     cudaEventElapsedTime(&t, p->ev0, p->ev1);
     for (int l = 0; l < nlevels; ++l) p->levels[l].n = (size_t)p->h_sched->n[l];
     if (p->h_sched->status == 1) return cp_fail(CP_ERR_CAPACITY, "graph engine: worklist level capacity exceeded");
+    if (p->h_cnt[C_ERR] & E_TC)
+        return cp_fail(CP_ERR_DEVICE, "graph engine: a tensor-core completion wait of the inline network timed out");
     if (p->h_sched->status != 0) return cp_fail(CP_ERR_DEVICE, "graph engine: scheduler stopped (status %d)",
                                                 p->h_sched->status);
     cp_engine_fill_report(p->h_cnt, r);

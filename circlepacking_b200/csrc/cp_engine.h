@@ -24,21 +24,16 @@ bool cp_model_collecting(cp_prover* p);
 cp_status cp_model_collect_chunk(cp_prover* p, int fam, const cpb::BoxList& in, size_t begin, size_t count,
                                  const double* tab_t, const double* tab_v, int tab_n, double tab_h);
 
-// Graph-mode hints: launches (into the stream being captured) the model's
-// inference over the current job of the device scheduler; hint buffers hold
-// up to `cap` boxes.
-namespace cpb {
-struct DevSched;
-}
-cp_status cp_model_graph_hints(cp_prover* p, int fam, const cpb::DevSched* sched, const cpb::BoxList* levels,
-                               size_t cap, uint8_t** axis, uint8_t** order);
-// Sizes the model's hint buffers for chunks of up to `cap` boxes (before capture).
-cp_status cp_model_reserve_hints(cp_prover* p, size_t cap);
-// The current hint buffer (part of the graph's identity: the graph holds its address).
-const void* cp_model_hint_buffer(cp_prover* p);
 // Persistent level kernels of the graph engine (cp_graph_fp64.cu / cp_graph_fp32.cu).
 void* cp_graph_kernel_fp64(int fam, int variant);
 void* cp_graph_kernel_fp32(int fam, int variant);
+// Persistent level kernels that run the proposal network inline (128 threads).
+void* cp_graph_kernel_net_fp64(int fam);
+void* cp_graph_kernel_net_fp32(int fam);
+// The trained network of a family for kernels that run it inline: BF16 views,
+// FP32 master parameters and the completion-wait limit (CP_ERR_INVALID when
+// the family has no model).
+cp_status cp_model_net_params(cp_prover* p, int fam, const void** views, const float** master, int* wait_limit);
 
 // Pieces of the refinement engine reused by the static-scratch entry point
 // (cp_noalloc.cu).  Counters: cp_engine_counter_words() 64-bit words.

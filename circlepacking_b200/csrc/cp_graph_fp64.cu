@@ -27,3 +27,14 @@ void* cp_graph_kernel_fp64(int fam, int variant) {
     default: return pick<5>(variant);
     }
 }
+
+void* cp_graph_kernel_net_fp64(int fam) {
+    switch (fam) {
+    case 0: return (void*)k_level_persist_net<0, 0>;
+    case 1: return (void*)k_level_persist_net<1, 0>;
+    case 2: return (void*)k_level_persist_net<2, 0>;
+    case 3: return (void*)k_level_persist_net<3, 0>;
+    case 4: return (void*)k_level_persist_net<4, 0>;
+    default: return (void*)k_level_persist_net<5, 0>;
+    }
+}

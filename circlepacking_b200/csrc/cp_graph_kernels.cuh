@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "cp_level.cuh"
+#include "cp_tc.cuh"
 
 namespace cpb {
 
@@ -65,6 +66,100 @@ __global__ void __launch_bounds__(BLOCK) __maxnreg__(graph_regs(BLOCK)) k_level_
             level_step<FAM, PREC>(a, (size_t)(j0 + (unsigned long long)lane), sm, handles);
         }
     }
+    level_flush(a, sm, handles);
+}
+
+// The persistent level kernel with the proposal network run inline: a CTA of
+// 128 threads claims 128 boxes of the job at a time, computes their features,
+// runs the network's forward pass on the tensor cores (tcgen05, accumulators in
+// 64 tensor-memory columns, tc::net_forward), and each thread evaluates its box
+// with the criterion order and split axis the network proposes.  The verdicts
+// are the interval kernels' own; a timed-out tensor-core wait raises E_TC.
+struct NetArgs {
+    const tc::bf16* views;
+    const float* master;
+    int wait_limit;
+    int want_order, want_axis;
+};
+constexpr int kNetBlock = tc::kTcRows;  // one box per thread of a 128-thread CTA
+constexpr int kNetMaxCtasPerSm = 512 / (int)tc::kNetCols;  // tensor memory: 512 columns per SM
+
+// (__launch_bounds__ with 5 resident CTAs caps the registers near the 96 of the
+// plain persistent kernel's 128-thread shape)
+template <int FAM, int PREC>
+__global__ void __launch_bounds__(kNetBlock, 5) k_level_persist_net(PersistArgs pa, NetArgs na) {
+    constexpr int D = family_dims(FAM);
+    __shared__ LevelSmem<kNetBlock / 32> sm;
+    __shared__ __align__(128) tc::NetSmem net;
+    __shared__ unsigned long long claim;
+    const DevJob job = pa.sched->job;
+    if (job.count == 0) return;  // uniform over the grid
+    LevelArgs a;
+    a.in = pa.levels[job.in_level];
+    a.begin = job.begin;
+    a.count = job.count;
+    a.out = job.out_level >= 0 ? pa.levels[job.out_level] : BoxList{nullptr, nullptr, nullptr, 0};
+    a.cnt = pa.cnt;
+    a.per_depth = pa.per_depth;
+    a.tab = pa.tab;
+    a.policy = pa.policy;
+    a.lambda_scale = pa.lambda_scale;
+    a.max_depth = job.out_level >= 0 ? pa.max_depth : 0;
+    a.axis_hint = nullptr;
+    a.order_hint = nullptr;
+    a.digest = pa.digest;
+    level_smem_init(sm);
+    tc::net_setup(net, na.views, na.master);
+    __syncthreads();
+    unsigned handles = 0;
+    bool ok = true;
+    for (;;) {
+        if (threadIdx.x == 0) claim = atomicAdd(&pa.sched->claim, (unsigned long long)kNetBlock);
+        __syncthreads();
+        const unsigned long long start = claim;
+        __syncthreads();  // every thread has read the claim before it is replaced
+        if (start >= job.count) break;  // uniform over the CTA
+        const size_t j = (size_t)(start + threadIdx.x);
+        float f[tc::NK];
+        if (j < job.count) {
+            const size_t i = a.begin + j;
+            double lo[4], hi[4];
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                lo[d] = a.in.lo[d * a.in.cap + i];
+                hi[d] = a.in.hi[d * a.in.cap + i];
+            }
+            const int dep = a.in.depth[i];
+            tc::box_features_fast<D>(lo, hi, dep == 0xFF ? 0 : dep, f);
+        } else {
+#pragma unroll
+            for (int k = 0; k < tc::NK; ++k) f[k] = 0.f;
+        }
+        float z[tc::NO];
+        if (!(ok = tc::net_forward(net, f, z, na.wait_limit))) break;
+        int ord = -1, ax = -1;
+        if (na.want_order) {
+            if (FAM == F_MIDDLE)
+                ord = fmaxf(z[2], z[3]) > fmaxf(z[0], z[1]) ? 1 : 0;
+            else if (FAM == F_END_2D || FAM == F_END_3D)
+                ord = z[1] > z[0] ? 1 : 0;
+            else
+                ord = 0;
+        }
+        if (na.want_axis) {
+            ax = 0;
+            float best = z[4];
+#pragma unroll
+            for (int d = 1; d < D; ++d)
+                if (z[4 + d] > best) {
+                    best = z[4 + d];
+                    ax = d;
+                }
+        }
+        level_step<FAM, PREC>(a, j, sm, handles, ord, ax);
+    }
+    if (!ok && threadIdx.x == 0) atomicOr(&a.cnt[C_ERR], (unsigned long long)E_TC);
+    tc::net_teardown(net, ok);
     level_flush(a, sm, handles);
 }
 

@@ -32,7 +32,7 @@ enum : int {
     C_DIGEST = 26,      // 2 words: sum and xor of the per-box verdict hashes (when enabled)
     C_COUNT = 28
 };
-enum : unsigned long long { E_OVERFLOW = 1, E_NOFIT = 2, E_TRAP = 4 };
+enum : unsigned long long { E_OVERFLOW = 1, E_NOFIT = 2, E_TRAP = 4, E_TC = 8 /* tensor-core wait timed out */ };
 constexpr int kDepthBins = 64;
 
 struct LevelArgs {
@@ -95,8 +95,11 @@ __device__ __forceinline__ void level_smem_init(LevelSmem<WARPS>& sm) {
 
 // One lane's box j of the chunk (j >= a.count: the lane only takes part in the
 // warp's collective child write).  All 32 lanes of the warp must call it.
+// ord_in / axis_in >= 0: this box's criterion order / split axis (SPLIT_GIVEN),
+// from a network run inline; otherwise the hint arrays (or the defaults).
 template <int FAM, int PREC, int WARPS>
-__device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSmem<WARPS>& sm, unsigned& handles) {
+__device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSmem<WARPS>& sm, unsigned& handles,
+                                           int ord_in = -1, int axis_in = -1) {
     constexpr int D = family_dims(FAM);
     const size_t i = a.begin + j;
     unsigned nchild = 0;
@@ -112,7 +115,7 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                 lo[d] = a.in.lo[d * a.in.cap + i];
                 hi[d] = a.in.hi[d * a.in.cap + i];
             }
-            const int ord = a.order_hint ? a.order_hint[j] : 0;
+            const int ord = ord_in >= 0 ? ord_in : (a.order_hint ? a.order_hint[j] : 0);
             int v;
             if (PREC == CP_FP32_PREFILTER) {
                 uint8_t pmask;
@@ -147,7 +150,7 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                     else if (a.policy == SPLIT_HYBRID)
                         axis = hybrid_axis<D>(lo, hi, a.lambda_scale);
                     else if (a.policy == SPLIT_GIVEN)
-                        axis = a.axis_hint ? (a.axis_hint[j] % D) : 0;
+                        axis = axis_in >= 0 ? axis_in % D : (a.axis_hint ? (a.axis_hint[j] % D) : 0);
                 }
             }
         }

@@ -31,25 +31,18 @@
 #include "cp_common.h"
 #include "cp_engine.h"
 #include "cp_level.cuh"
+#include "cp_tc.cuh"
 
 using namespace cpb;
 
 namespace {
 
-constexpr int NIN = 9, NK = 16, NH = 64, NO = 8;
-// flat FP32 parameters: W1 [16][64] (in x out), b1, W2 [64][64], b2, W3 [64][8], b3
-constexpr int P_W1 = 0, P_B1 = P_W1 + NK * NH, P_W2 = P_B1 + NH, P_B2 = P_W2 + NH * NH, P_W3 = P_B2 + NH,
-              P_B3 = P_W3 + NH * NO, NPARAM = P_B3 + NO;
-// BF16 views in the layouts the fragments read: W1T [64][16], W2T [64][64],
-// W3T [8][64] (out x in), W2 [64][64], W3 [64][8] (in x out)
-constexpr int V_W1T = 0, V_W2T = V_W1T + NH * NK, V_W3T = V_W2T + NH * NH, V_W2 = V_W3T + NO * NH,
-              V_W3 = V_W2 + NH * NH, NVIEW = V_W3 + NH * NO;
+using namespace cpb::tc;
+
 // shared-memory pitches (elements) chosen so fragment loads are bank-conflict free
 constexpr int PK = 24, PH = 72;
 constexpr int kRowsPerWarp = 16, kTrainWarps = 4, kTrainRows = kRowsPerWarp * kTrainWarps;
-constexpr float kGeluC = 0.7978845608028654f;
 
-using bf16 = __nv_bfloat16;
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -70,13 +63,6 @@ __device__ __forceinline__ void mma16816(float* d, const uint32_t* a, uint32_t b
 
 __device__ __forceinline__ float gelu(float x) {
     const float t = tanhf(kGeluC * (x + 0.044715f * x * x * x));
-    return 0.5f * x * (1.0f + t);
-}
-// Inference GELU: the hardware tanh approximation (tanh.approx.f32, one MUFU
-// operation; maximum relative error about 2^-11), which is below BF16 resolution.
-__device__ __forceinline__ float gelu_fast(float x) {
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(kGeluC * (x + 0.044715f * x * x * x)));
     return 0.5f * x * (1.0f + t);
 }
 __device__ __forceinline__ float gelu_grad(float x) {
@@ -105,28 +91,6 @@ __device__ __forceinline__ void box_features(const double* lo, const double* hi,
     for (int k = 9; k < 16; ++k) f[k] = 0.f;
 }
 
-// The same features in single precision (inference): the relative width is
-// clamped at 2^-64, far inside FP32 range, so FP32 log2 loses nothing at BF16
-// resolution.
-template <int D>
-__device__ __forceinline__ void box_features_fast(const double* lo, const double* hi, int depth, float* f) {
-#pragma unroll
-    for (int d = 0; d < 4; ++d) {
-        if (d < D) {
-            const float a = d == 0 ? 0.5f : 0.0f, inv = d == 0 ? (1.0f / 0.49f) : 4.0f;
-            const float c = (float)(0.5 * (lo[d] + hi[d]));
-            const float w = fmaxf((float)(hi[d] - lo[d]) * inv, 5.421010862427522e-20f);  // 2^-64
-            f[2 * d] = (c - a) * inv * 2.0f - 1.0f;
-            f[2 * d + 1] = __log2f(w) * (1.0f / 16.0f) + 1.0f;
-        } else {
-            f[2 * d] = 0.f;
-            f[2 * d + 1] = 0.f;
-        }
-    }
-    f[8] = (float)depth / 32.0f;
-#pragma unroll
-    for (int k = 9; k < 16; ++k) f[k] = 0.f;
-}
 
 // Shared-memory copies of the forward weights.
 struct FwdSmem {
@@ -533,8 +497,6 @@ __global__ void k_adam(float* __restrict__ master, float* __restrict__ m, float*
 struct InferArgs {
     BoxList in;
     size_t begin, count;
-    const DevSched* sched;   // graph mode: take in/begin/count from the scheduler's job
-    const BoxList* levels;
     const bf16* views;
     const float* master;
     uint8_t* axis;     // per box, indexed from `begin` (may be null)
@@ -554,13 +516,6 @@ template <int FAM>
 __global__ void __launch_bounds__(128) k_infer(InferArgs a) {
     constexpr int D = family_dims(FAM);
     __shared__ InferSmem s;
-    if (a.sched) {
-        const DevJob job = a.sched->job;
-        if (job.count == 0) return;
-        a.in = a.levels[job.in_level];
-        a.begin = job.begin;
-        a.count = job.count;
-    }
     load_fwd(s.f, a.views, a.master);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -632,7 +587,6 @@ __global__ void __launch_bounds__(128) k_infer(InferArgs a) {
 // GELU, and writes the next layer's operand tile.  Waits on the MMA-completion
 // mbarrier are bounded: on time-out the kernel raises *err, waits (bounded)
 // once more, frees its tensor memory and returns.
-constexpr int kTcRows = 128;
 constexpr uint32_t kTcCols = 128;  // tensor-memory columns per CTA: [0, 64) hidden, [64, 80) logits
 
 struct TcSmem {
@@ -644,62 +598,6 @@ struct TcSmem {
     unsigned long long mbar;
     uint32_t tmem;
 };
-
-// element offset of (row, k) in a K-major core-matrix tile with K columns
-__device__ __forceinline__ int cm_off(int row, int k, int K) {
-    return (row >> 3) * (K * 8) + (k >> 3) * 64 + (row & 7) * 8 + (k & 7);
-}
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-// shared-memory matrix descriptor (no swizzle, K-major), Blackwell version 1
-__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
-}
-// instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128
-__host__ __device__ constexpr uint32_t tc_idesc(int n) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
-}
-__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
-        :
-        : "r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc)
-        : "memory");
-}
-__device__ __forceinline__ void tc_commit(uint32_t mbar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
-                 : "memory");
-}
-constexpr int kTcWaitLimit = 1 << 22;  // default polls of a bounded completion wait
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, int limit = kTcWaitLimit) {
-    for (int it = 0; it < limit; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(mbar), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_ld64(uint32_t taddr, uint32_t* r) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
-                 : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t* r) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                 : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
 
 struct TcArgs {
     InferArgs a;
@@ -889,12 +787,6 @@ struct TtSmem {
     uint32_t tmem;
 };
 
-__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t* r) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                 : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
 
 // D (tensor memory, column dcol) = A (128 x K tile) * B (N x K tile)^T, K = 16 * ksteps
 __device__ __forceinline__ void tt_gemm(uint32_t tmem, uint32_t dcol, const bf16* A, const bf16* B, int K, int N) {
@@ -1248,7 +1140,9 @@ struct ModelState {
     uint8_t* rec_depth = nullptr;
     unsigned long long* rec_count = nullptr;
     // inference kernel: 0 = warp-level mma.sync, 1 = tcgen05 with tensor memory
-    int infer_kind = 0;
+    // (default: the same forward pass the graph engine's level kernel runs inline,
+    // so both engines take identical learned decisions)
+    int infer_kind = 1;
     int* tc_err = nullptr;    // device flag raised by a timed-out tcgen05 wait
     int* tc_err_h = nullptr;  // pinned copy, refreshed after every tcgen05 launch
     int tc_wait_limit = kTcWaitLimit;
@@ -1378,20 +1272,6 @@ cp_status launch_infer_t(const InferArgs& a, cudaStream_t st) {
     k_infer<FAM><<<grid, 128, 0, st>>>(a);
     return cp_check_launch();
 }
-template <int FAM>
-void k_inferv_t(const InferArgs& a, cudaStream_t st) {
-    k_infer<FAM><<<148 * 4, 128, 0, st>>>(a);
-}
-void k_inferv(int fam, const InferArgs& a, cudaStream_t st) {
-    switch (fam) {
-    case 0: k_inferv_t<0>(a, st); break;
-    case 1: k_inferv_t<1>(a, st); break;
-    case 2: k_inferv_t<2>(a, st); break;
-    case 3: k_inferv_t<3>(a, st); break;
-    case 4: k_inferv_t<4>(a, st); break;
-    default: k_inferv_t<5>(a, st); break;
-    }
-}
 cp_status launch_infer(int fam, const InferArgs& a, cudaStream_t st) {
     switch (fam) {
     case 0: return launch_infer_t<0>(a, st);
@@ -1443,7 +1323,7 @@ cp_status launch_label(int fam, const LabelArgs& a, cudaStream_t st) {
 // the previous launch is checked first and this launch's flag is copied to
 // pinned memory behind it (the engine synchronises the stream between chunks).
 cp_status run_infer(ModelState* m, int fam, const InferArgs& a, cudaStream_t st) {
-    if (m->infer_kind == 0 || a.sched) return launch_infer(fam, a, st);
+    if (m->infer_kind == 0) return launch_infer(fam, a, st);
     if (!m->tc_err) {
         M_TRY(ok_or(cudaMalloc(&m->tc_err, sizeof(int))));
         M_TRY(ok_or(cudaMallocHost(&m->tc_err_h, sizeof(int))));
@@ -1480,8 +1360,6 @@ cp_status cp_model_hints(cp_prover* p, int fam, const BoxList& in, size_t begin,
     a.count = count;
     a.views = m->fam[fam].views;
     a.master = m->fam[fam].master;
-    a.sched = nullptr;
-    a.levels = nullptr;
     a.axis = axis ? m->hint_axis : nullptr;
     a.order = order ? m->hint_order : nullptr;
     a.logits = nullptr;
@@ -1491,51 +1369,14 @@ cp_status cp_model_hints(cp_prover* p, int fam, const BoxList& in, size_t begin,
     return CP_OK;
 }
 
-cp_status cp_model_graph_hints(cp_prover* p, int fam, const DevSched* sched, const BoxList* levels, size_t cap,
-                               uint8_t** axis, uint8_t** order) {
+cp_status cp_model_net_params(cp_prover* p, int fam, const void** views, const float** master, int* wait_limit) {
     ModelState* m = state(p, false);
-    if (!m || !m->fam[fam].ready)
+    if (!m || fam < 0 || fam > 5 || !m->fam[fam].ready)
         return cp_fail(CP_ERR_INVALID, "no proposal model for family %d: train one (cp_model_train) or load "
                                        "parameters (cp_model_set_params)", fam);
-    if (m->hint_cap < cap) {
-        // allocation is not allowed during stream capture: callers size the
-        // buffers before capturing (cp_model_reserve_hints)
-        return cp_fail(CP_ERR_INVALID, "hint buffers not reserved for %zu boxes", cap);
-    }
-    InferArgs a;
-    a.in = BoxList{nullptr, nullptr, nullptr, 0};
-    a.begin = 0;
-    a.count = 0;
-    a.sched = sched;
-    a.levels = levels;
-    a.views = m->fam[fam].views;
-    a.master = m->fam[fam].master;
-    a.axis = axis ? m->hint_axis : nullptr;
-    a.order = order ? m->hint_order : nullptr;
-    a.logits = nullptr;
-    // grid independent of the (device-side) count: one resident wave
-    k_inferv(fam, a, cp_prover_stream(p));
-    M_TRY(cp_check_launch());
-    if (axis) *axis = m->hint_axis;
-    if (order) *order = m->hint_order;
-    return CP_OK;
-}
-
-const void* cp_model_hint_buffer(cp_prover* p) {
-    ModelState* m = state(p, false);
-    return m ? (const void*)m->hint_axis : nullptr;
-}
-
-cp_status cp_model_reserve_hints(cp_prover* p, size_t cap) {
-    ModelState* m = state(p, false);
-    if (!m) return CP_OK;
-    if (m->hint_cap >= cap) return CP_OK;
-    cudaFree(m->hint_axis);
-    m->hint_axis = nullptr;
-    m->hint_cap = 0;
-    M_TRY(ok_or(cudaMalloc(&m->hint_axis, 2 * cap)));
-    m->hint_order = m->hint_axis + cap;
-    m->hint_cap = cap;
+    *views = m->fam[fam].views;
+    *master = m->fam[fam].master;
+    *wait_limit = m->tc_wait_limit;
     return CP_OK;
 }
 
@@ -1825,8 +1666,6 @@ cp_status cp_model_predict(cp_prover* p, int family, const double* lo, const dou
             a.in = BoxList{dlo, dhi, dd, n};
             a.begin = 0;
             a.count = n;
-            a.sched = nullptr;
-            a.levels = nullptr;
             a.views = m->fam[family].views;
             a.master = m->fam[family].master;
             a.axis = dax;

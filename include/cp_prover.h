@@ -398,10 +398,12 @@ cp_status cp_model_loss_grad_kind(int kind, int family, const float* params, con
 /* The kernel cp_model_train runs: 1 = tcgen05 (default), 0 = mma.sync. */
 cp_status cp_model_set_training(cp_prover* p, int kind);
 
-/* The kernel that runs the network for hints and predictions: 0 = warp-level
- * BF16 mma.sync (default; also the one used inside the graph engine),
- * 1 = tcgen05.mma with FP32 accumulators in tensor memory, 128 boxes per CTA
- * (bounded completion waits; a time-out returns CP_ERR_DEVICE). */
+/* The kernel that runs the network for hints and predictions of the
+ * host-driven level loop and cp_model_predict: 1 = tcgen05.mma with FP32
+ * accumulators in tensor memory, 128 boxes per CTA (default; the same forward
+ * pass the graph engine's level kernel runs inline, so both engines take the
+ * same learned decisions), 0 = warp-level BF16 mma.sync.  Bounded completion
+ * waits; a time-out returns CP_ERR_DEVICE. */
 cp_status cp_model_set_inference(cp_prover* p, int kind);
 
 /* Diagnostics: polls per bounded completion wait of the tcgen05 inference

@@ -24,6 +24,7 @@
 #include <cstdint>
 #include <cstring>
 #include <queue>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -853,6 +854,107 @@ int orc_eval_boxes(int fam, const double* lo, const double* hi, int64_t n, int64
     return 0;
 }
 
+// The box refinement of the device engine with the uniform split (every axis
+// bisected), restated on the CPU for the boxes below a sample of lattice seed
+// boxes, on the reference kernel's own evaluation path (stop at the first
+// failing sub-check and handle, and at a firing fit check where the kernel
+// traps).  A box that is neither proved nor empty is unresolved at max_depth,
+// else its 2^dims children (midpoints rounded to nearest) are intersected with
+// the dependent ranges of their own lambda interval (single-placement bound from
+// the same 2^16-point lambda grid as the device: the value at the largest grid
+// point <= lambda.lb) and evaluated in turn; children with an empty range are
+// dropped (clipped).  out[0..4]: verdict counts, out[5] unresolved, out[6]
+// clipped; per_depth[d] evaluated boxes at depth d < 16; ops[4 d + k]
+// primitive counts (add, mul, div, asin) at depth d < 16 (may be NULL).
+struct SingleGrid {
+    std::vector<double> t, v;
+    double h = 0.0;
+};
+static const SingleGrid& single_grid() {
+    static SingleGrid g = [] {
+        SingleGrid s;
+        const int n = 1 << 16;
+        s.h = (kLambdaMax - kLambdaMin) / (n - 1);
+        s.t.resize(n);
+        s.v.resize(n);
+        parallel_for(n, 0, [&](int64_t b, int64_t e, int) {
+            for (int64_t i = b; i < e; ++i) {
+                s.t[i] = std::fma((double)i, s.h, kLambdaMin);
+                s.v[i] = single_placement(s.t[i]);
+            }
+        });
+        return s;
+    }();
+    return g;
+}
+static double single_upper(const SingleGrid& g, double la_lo) {
+    if (!(la_lo >= g.t[0])) return 0.25;
+    int64_t i = (int64_t)((la_lo - g.t[0]) / g.h);
+    const int64_t n = (int64_t)g.t.size();
+    if (i >= n) i = n - 1;
+    while (i > 0 && g.t[i] > la_lo) --i;
+    while (i + 1 < n && g.t[i + 1] <= la_lo) ++i;
+    return g.v[i];
+}
+static bool clip_child(int fam, const SingleGrid& g, double* lo, double* hi) {
+    const Iv la{lo[0], hi[0]};
+    const Iv r1r = range_r1(la, single_upper(g, la.lb));
+    if (lo[1] < r1r.lb) lo[1] = r1r.lb;
+    if (r1r.ub < hi[1]) hi[1] = r1r.ub;
+    if (lo[1] > hi[1]) return false;
+    const Iv r2r = range_r2(fam, la, Iv{lo[1], hi[1]});
+    if (lo[2] < r2r.lb) lo[2] = r2r.lb;
+    if (r2r.ub < hi[2]) hi[2] = r2r.ub;
+    if (lo[2] > hi[2]) return false;
+    if (family_dims(fam) == 4) {
+        const Iv r3r = range_r3(fam, la, Iv{lo[2], hi[2]});
+        if (lo[3] < r3r.lb) lo[3] = r3r.lb;
+        if (r3r.ub < hi[3]) hi[3] = r3r.ub;
+        if (lo[3] > hi[3]) return false;
+    }
+    return true;
+}
+struct RefineTally {
+    int64_t out[7] = {0, 0, 0, 0, 0, 0, 0};
+    int64_t per_depth[16] = {0};
+    OpCount ops[16] = {};
+};
+static void refine_box(int fam, const SingleGrid& g, const double* lo, const double* hi, int depth, int max_depth,
+                       RefineTally& t) {
+    const int dims = family_dims(fam);
+    const int dd = depth < 16 ? depth : 15;
+    Out o;
+    OpCount c{0, 0, 0, 0};
+    t_count = &c;
+    eval_box(fam, lo, hi, o);
+    t_count = nullptr;
+    t.ops[dd].add += c.add;
+    t.ops[dd].mul += c.mul;
+    t.ops[dd].div += c.div;
+    t.ops[dd].asin += c.asin;
+    t.out[o.verdict]++;
+    t.per_depth[dd]++;
+    if (o.verdict == V_PROVED || o.verdict == V_EMPTY) return;
+    if (depth >= max_depth) {
+        t.out[5]++;
+        return;
+    }
+    double mid[4];
+    for (int d = 0; d < dims; ++d) mid[d] = 0.5 * (lo[d] + hi[d]);
+    for (int k = 0; k < (1 << dims); ++k) {
+        double cl[4], ch[4];
+        for (int d = 0; d < dims; ++d) {
+            cl[d] = ((k >> d) & 1) ? mid[d] : lo[d];
+            ch[d] = ((k >> d) & 1) ? hi[d] : mid[d];
+        }
+        if (!clip_child(fam, g, cl, ch)) {
+            t.out[6]++;
+            continue;
+        }
+        refine_box(fam, g, cl, ch, depth + 1, max_depth, t);
+    }
+}
+
 // Count the primitive operations of the evaluation of n boxes.
 // counts[0..3] = add/sub, mul, div, asin (summed over the boxes).  decide = 0:
 // every sub-criterion (FULL); decide = 1: the reference kernel's own path, which
@@ -883,6 +985,67 @@ int orc_count_ops_mode(int fam, const double* lo, const double* hi, int64_t n, i
 }
 int orc_count_ops(int fam, const double* lo, const double* hi, int64_t n, int64_t stride, uint64_t* counts) {
     return orc_count_ops_mode(fam, lo, hi, n, stride, 0, counts);
+}
+
+// The uniform refinement below the lattice seed boxes idx[0..n) of a family
+// lattice (see refine_box), over nthreads host threads (0 = all).
+int orc_refine_sample(int fam, double outer_lb, double outer_ub, const int32_t* sizes, const int64_t* idx, int64_t n,
+                      int max_depth, int64_t* out, int64_t* per_depth, uint64_t* ops, int nthreads) {
+    if (fam < 0 || fam > 5 || n < 0 || max_depth < 0 || max_depth > 15 || !out) return 1;
+    LatticeSpec s{fam, {sizes[0], sizes[1], sizes[2], family_dims(fam) == 4 ? sizes[3] : 1},
+                  {outer_lb, outer_ub}, true};
+    const SingleGrid& g = single_grid();
+    int nt = nthreads > 0 ? nthreads : (int)std::thread::hardware_concurrency();
+    if (nt < 1) nt = 1;
+    std::vector<RefineTally> tally((size_t)nt);
+    // the lattice kernels' own single-placement bound per lambda slab (exact, as the seed)
+    std::vector<double> single(s.n[0], -1.0);
+    std::vector<std::once_flag> once(s.n[0]);
+    const int dims = family_dims(fam);
+    // small work items: one seed box each (the trees below seeds differ widely in size)
+    std::atomic<int64_t> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t) {
+        pool.emplace_back([&, t] {
+            t_decide = true;
+            int ix[4] = {0, 0, 0, 0};
+            double l[4], h[4];
+            for (;;) {
+                const int64_t i = next.fetch_add(1);
+                if (i >= n) break;
+                unravel(s, idx[i], ix);
+                std::call_once(once[ix[0]], [&] {
+                    single[ix[0]] = single_placement(subinterval(s.outer, ix[0], s.n[0], s.fused).lb);
+                });
+                if (!lattice_box(s, ix, single[ix[0]], l, h)) {
+                    tally[t].out[6]++;
+                    continue;
+                }
+                refine_box(fam, g, l, h, 0, max_depth, tally[t]);
+            }
+            t_decide = false;
+        });
+    }
+    for (auto& th : pool) th.join();
+    for (int k = 0; k < 7; ++k) out[k] = 0;
+    for (int d = 0; d < 16; ++d) {
+        if (per_depth) per_depth[d] = 0;
+        if (ops) ops[4 * d] = ops[4 * d + 1] = ops[4 * d + 2] = ops[4 * d + 3] = 0;
+    }
+    for (const auto& ta : tally) {
+        for (int k = 0; k < 7; ++k) out[k] += ta.out[k];
+        for (int d = 0; d < 16; ++d) {
+            if (per_depth) per_depth[d] += ta.per_depth[d];
+            if (ops) {
+                ops[4 * d] += ta.ops[d].add;
+                ops[4 * d + 1] += ta.ops[d].mul;
+                ops[4 * d + 2] += ta.ops[d].div;
+                ops[4 * d + 3] += ta.ops[d].asin;
+            }
+        }
+    }
+    (void)dims;
+    return 0;
 }
 
 double orc_single_placement(double lb_lambda) { return single_placement(lb_lambda); }

@@ -43,6 +43,7 @@ def lib():
         L.orc_eval_boxes.argtypes = [I32, P, P, I64, I64, P, P, P, I32]
         L.orc_count_ops.argtypes = [I32, P, P, I64, I64, P]
         L.orc_count_ops_mode.argtypes = [I32, P, P, I64, I64, I32, P]
+        L.orc_refine_sample.argtypes = [I32, D, D, P, P, I64, I32, P, P, P, I32]
         L.orc_single_placement.argtypes = [D]
         L.orc_single_placement.restype = D
         L.orc_asin_pad.argtypes = [P, I64, P, P]
@@ -86,6 +87,25 @@ def count_ops(family: int, lo: np.ndarray, hi: np.ndarray, decide: bool = False)
     c = np.zeros(4, np.uint64)
     lib().orc_count_ops_mode(family, _p(lo), _p(hi), lo.shape[1], lo.shape[1], int(decide), _p(c))
     return dict(add=int(c[0]), mul=int(c[1]), div=int(c[2]), asin=int(c[3]), boxes=int(lo.shape[1]))
+
+
+def refine_sample(family: int, sizes, idx, max_depth: int, outer=(0.5, 0.9900000000000001), threads: int = 0) -> dict:
+    """The device engine's uniform refinement below the lattice seed boxes `idx`
+    of the lattice `sizes` over `outer`, restated on the CPU on the reference
+    kernel's own evaluation path: verdict counts, unresolved, clipped, boxes
+    evaluated per depth and primitive operations (add, mul, div, asin) per depth."""
+    s = np.zeros(4, np.int32)
+    s[: len(sizes)] = sizes
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    out = np.zeros(7, np.int64)
+    per_depth = np.zeros(16, np.int64)
+    ops = np.zeros((16, 4), np.uint64)
+    rc = lib().orc_refine_sample(family, float(outer[0]), float(outer[1]), _p(s), _p(idx), idx.size, max_depth,
+                                 _p(out), _p(per_depth), _p(ops), threads)
+    if rc:
+        raise ValueError("orc_refine_sample: bad arguments")
+    return dict(verdicts=out[:5].tolist(), unresolved=int(out[5]), clipped=int(out[6]),
+                evaluated=int(out[:5].sum()), per_depth=per_depth.tolist(), ops=ops.astype(np.int64))
 
 
 def single_placement(lb_lambda: float) -> float:

@@ -128,3 +128,30 @@ def test_autotune_variants_keep_verdicts(cp, prover, family):
         prover.set_level_variant(family, cp.FP64, v)
         outs.append(prover.refine(family, **kw))
     assert all(o["verdicts"] == outs[0]["verdicts"] and o["unresolved"] == outs[0]["unresolved"] for o in outs)
+
+
+@pytest.mark.parametrize("family", range(6))
+def test_cpu_restated_refinement_matches_device(cp, oracle, family):
+    """The CPU restatement of the uniform refinement (the bench's CPU baseline
+    workload) evaluates the same tree as the device engine below the same seed
+    boxes: equal boxes per depth and verdict counts, up to the rare boxes whose
+    criteria sit within the host-libm / CUDA asin difference of a threshold."""
+    dims = cp.DIMS[family]
+    sizes = [64] * dims
+    idx = np.sort(np.random.default_rng(40 + family).choice(64 ** dims, 300, replace=False))
+    want = oracle.refine_sample(family, sizes, idx, 2)
+    lo, hi, vis = cp.lattice_boxes(family, (cp.LAMBDA_MIN, cp.LAMBDA_MAX), sizes, idx, visited=True)
+    import torch
+
+    dp = torch.where(vis != 0, 0, 255).to(torch.uint8)
+    p = cp.Prover(0)
+    try:
+        got = p.refine_boxes(family, lo, hi, depth=dp, policy=cp.SPLIT_UNIFORM, max_depth=2)
+    finally:
+        p.close()
+    for d in range(3):
+        a, b = want["per_depth"][d], got["per_depth"][d] if d < len(got["per_depth"]) else 0
+        assert abs(a - b) <= 1e-3 * max(a, b) + 2, (d, a, b)
+    for v in range(5):
+        a, b = want["verdicts"][v], got["verdicts"][v]
+        assert abs(a - b) <= 1e-3 * max(a, b) + 2, (v, a, b)
