@@ -79,6 +79,8 @@ def parse():
     ap.add_argument("--uneven-family", type=int, default=3, help="family of the uneven-depth worklist legs")
     ap.add_argument("--uneven-random", type=int, default=10_000_000, help="random boxes added to the lattice seed")
     ap.add_argument("--no-fp32-leg", action="store_true", help="skip the FP32 pre-pass form of the whole step")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="with --no-autotune: the precision of the graph-engine form (profiling runs)")
     return ap.parse_args()
 
 
@@ -261,49 +263,42 @@ def train_models(prover, cp, depth):
 TRAFFIC_PER_BOX, ALGORITHMIC_BYTES_PER_BOX = 2.391e9 / 11.95e6, 124.0
 FP64_PIPE_ACTIVE_NCU = 0.209
 
-# lambda-only proofs: the radius resolution of the seed each family needs
-PROOF_SEEDS = {1: (64, 32, 32), 2: (64, 64, 64, 16), 3: (64, 32, 32, 8), 4: (64, 128, 128), 5: (64, 32, 32, 8)}
-PROOF_DEPTH = 24
-PROOF_FAMILIES = (1, 2, 3, 4, 5)
+PROOF_FAMILIES = (0, 1, 2, 3, 4, 5)
 
 
 def proof_leg(prover, cp, forms, families, world=1):
-    """Full-domain proofs: the family's whole domain (lambda in [0.5, 0.99], the
-    dependent radius ranges) from a lattice seed with 64 lambda slabs and the
-    radius resolution the family needs (PROOF_SEEDS), not-proved boxes bisected
-    in lambda only -- the reference's own refinement rule
-    (run_kernel.cuh:110-127) -- down to depth 24.  A family is proved when no box
-    is left unresolved.  Both forms evaluate the same tree of boxes, so their
-    verdict counts must be identical; the best form runs it as one graph launch."""
+    """Full-domain proofs by the library's proof driver (cp_prove_family with
+    cp_proof_defaults): each family's whole domain (lambda in [0.5, 0.99], the
+    dependent radius ranges) from lattice seeds with the radius resolution the
+    family needs -- for start, lambda slabs narrowing geometrically toward 0.99,
+    each seeded with the reference's own radius lattice -- not-proved boxes
+    bisected in lambda only (the reference's own refinement rule,
+    run_kernel.cuh:110-127).  A family is proved when no box is left
+    unresolved.  The best form runs every slab as one graph launch, the plain
+    form as the FP64 host-driven level loop; both evaluate the same tree, which
+    the per-box verdict digests confirm."""
     out = []
     for f in families:
-        kw = dict(policy=cp.SPLIT_LAMBDA, max_depth=PROOF_DEPTH, seed_sizes=list(PROOF_SEEDS[f]),
-                  seed_lambda=SHARD, level_capacity=1 << 23, seed_part=PART, seed_parts=PARTS)
-        best_kw = dict(kw, precision=forms[f]["precision"], engine=cp.ENGINE_GRAPH,
-                       learned_order=forms[f].get("learned_order", False))
-        # the graph engine suits the proof's many small chunks; shape as tuned
-        plain_kw = dict(kw, precision=cp.FP64, engine=cp.ENGINE_LEVELS)
-        prover.refine(f, **best_kw)  # warm-up (graph build)
-        t0 = time.perf_counter()
-        b = prover.refine(f, **best_kw)
-        tb = time.perf_counter() - t0
         prover.set_level_variant(f, cp.FP64, 0)
-        prover.refine(f, **plain_kw)
-        t0 = time.perf_counter()
-        p = prover.refine(f, **plain_kw)
-        tp = time.perf_counter() - t0
-        # verdict identity box by box: one more run of each form with the digest on
-        same = same_boxes_and_verdicts(prover.refine(f, digest=True, **best_kw),
-                                       prover.refine(f, digest=True, **plain_kw))
-        # over all ranks' lambda pieces: counts summed, times the slowest rank's
+        # each rank refines its interleaved piece of every slab's lattice
+        best_kw = dict(engine=cp.ENGINE_GRAPH, precision=forms[f]["precision"], digest=1, seed_parts=PARTS,
+                       seed_part=PART)
+        plain_kw = dict(best_kw, engine=cp.ENGINE_LEVELS, precision=cp.FP64)
+        prover.prove_family(f, **dict(best_kw, slabs=1, seed_sizes=[4, 4, 4, 4]))  # warm-up (graph build)
+        b = prover.prove_family(f, **best_kw)
+        p = prover.prove_family(f, **plain_kw)
+        same = (b["digest"] == p["digest"] and b["verdicts"] == p["verdicts"] and b["per_depth"] == p["per_depth"]
+                and b["unresolved"] == p["unresolved"])
         unresolved = sum_over_ranks(world, b["unresolved"] + p["unresolved"])
+        d = prover.proof_defaults(f)
         out.append({"family": cp.FAMILIES[f], "proved": unresolved == 0,
-                    "boxes": int(sum_over_ranks(world, b["evaluated"])), "max_depth": len(b["per_depth"]) - 1,
-                    "best_wall_ms": max_over_ranks(world, tb * 1e3),
+                    "seeds": {"slabs": d["slabs"], "geometric": bool(d["geometric"]),
+                              "lattice_per_slab": d["seed_sizes"][:DIMS[f]], "max_depth": d["max_depth"]},
+                    "boxes": int(sum_over_ranks(world, b["evaluated"])), "max_depth": b["max_depth_seen"],
+                    "best_wall_ms": max_over_ranks(world, b["wall_ms"]),
                     "best_device_ms": max_over_ranks(world, b["device_ms"]),
-                    "plain_wall_ms": max_over_ranks(world, tp * 1e3),
+                    "plain_wall_ms": max_over_ranks(world, p["wall_ms"]),
                     "plain_device_ms": max_over_ranks(world, p["device_ms"]),
-                    "plain_launches": p["launches"],
                     "verdicts_identical": sum_over_ranks(world, 0 if same else 1) == 0})
     return out
 
@@ -364,9 +359,9 @@ def roofline_of(cp, device, reps, counts) -> dict:
                             f"step's {boxes} evaluated boxes",
             "kernel": "k_level_persist<family, precision, block> (per-box criteria + split), graph engine",
             "work_model": "per evaluated box: the reference kernel's own add/sub, mul, div and asin count (it stops "
-                          "at the first failing sub-check and handle), from the CPU restatement's op-counting mode on "
-                          "device-recorded samples of the step's boxes, per depth; each primitive counts 1 against "
-                          "the FP64 instruction peak (DFMA per lane per cycle)",
+                          "at the first failing sub-check and handle), counted by the CPU restatement while it refines "
+                          "sampled seeds of the same workload, per family and depth, weighted by the step's boxes per "
+                          "depth; each primitive counts 1 against the FP64 instruction peak (DFMA per lane per cycle)",
             "ops_per_second": {k: v / kernel_s / 1e12 for k, v in ops.items()} | {"unit": "T/s"},
             "frac_weighted_ddiv_rd": weighted(rates["ddiv_rd"]) / kernel_s / peak,
             "frac_weighted_library_div": weighted(rates["div_rd_lib"]) / kernel_s / peak,
@@ -568,8 +563,9 @@ def main():
     # ---- outside the timed region: proposal networks, kernel shapes, precisions
     models = None
     if args.no_autotune:
-        forms = {f: {"precision": FP64, "engine": cp.ENGINE_GRAPH} for f in FAMILIES}
-        tuning = {cp.FAMILIES[f]: {"precision": "fp64", "engine": "graph"} for f in FAMILIES}
+        prec = FP64 if args.precision == "fp64" else cp.FP32_PREFILTER
+        forms = {f: {"precision": prec, "engine": cp.ENGINE_GRAPH} for f in FAMILIES}
+        tuning = {cp.FAMILIES[f]: {"precision": args.precision, "engine": "graph"} for f in FAMILIES}
     else:
         if not args.no_learned:
             models = train_models(prover, cp, args.depth)

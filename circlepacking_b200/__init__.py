@@ -222,6 +222,31 @@ class ReferenceReport(ctypes.Structure):
                     wall_ms=self.wall_ms)
 
 
+class ProofOpts(ctypes.Structure):
+    _fields_ = [("family", ctypes.c_int32), ("precision", ctypes.c_int32), ("engine", ctypes.c_int32),
+                ("policy", ctypes.c_int32), ("max_depth", ctypes.c_int32), ("slabs", ctypes.c_int32),
+                ("geometric", ctypes.c_int32), ("seed_sizes", ctypes.c_int32 * 4), ("level_capacity", ctypes.c_int64),
+                ("digest", ctypes.c_int32), ("seed_parts", ctypes.c_int32), ("seed_part", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: (list(getattr(self, k)) if k == "seed_sizes" else getattr(self, k)) for k, _ in self._fields_}
+
+
+class ProofReport(ctypes.Structure):
+    _fields_ = [("proved", ctypes.c_int32), ("slabs_done", ctypes.c_int32), ("evaluated", ctypes.c_int64),
+                ("verdicts", ctypes.c_int64 * 5), ("unresolved", ctypes.c_int64), ("clipped", ctypes.c_int64),
+                ("per_depth", ctypes.c_int64 * 64), ("max_depth_seen", ctypes.c_int32),
+                ("first_unresolved_slab", ctypes.c_int32), ("device_ms", ctypes.c_double), ("wall_ms", ctypes.c_double),
+                ("digest", ctypes.c_uint64 * 2)]
+
+    def as_dict(self) -> dict:
+        return dict(proved=bool(self.proved), slabs_done=self.slabs_done, evaluated=self.evaluated,
+                    verdicts=list(self.verdicts), unresolved=self.unresolved, clipped=self.clipped,
+                    per_depth=list(self.per_depth)[: self.max_depth_seen + 1], max_depth_seen=self.max_depth_seen,
+                    first_unresolved_slab=self.first_unresolved_slab, device_ms=self.device_ms, wall_ms=self.wall_ms,
+                    digest=(int(self.digest[0]), int(self.digest[1])))
+
+
 def _declare_handle(L):
     P, I, D, SZ, I64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t, ctypes.c_int64
     L.cp_create.argtypes = [I, ctypes.POINTER(P)]
@@ -247,6 +272,11 @@ def _declare_handle(L):
     L.cp_autotune_graph.argtypes = [P, ctypes.POINTER(RefineOpts), ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_int), P]
     L.cp_random_boxes.argtypes = [P, I, ctypes.c_uint64, I, SZ, P, P, P]
+    L.cp_proof_defaults.argtypes = [I, ctypes.POINTER(ProofOpts)]
+    L.cp_prove_family.argtypes = [P, ctypes.POINTER(ProofOpts), ctypes.POINTER(ProofReport)]
+    L.cp_prove_all.argtypes = [P, I, I, ctypes.POINTER(ProofReport)]
+    L.cp_set_chunk_callback.argtypes = [P, P, P]
+    L.cp_set_chunk_callback.restype = None
 
 
 def measure_primitives(device: int = 0) -> dict:
@@ -306,6 +336,18 @@ class Prover:
 
     def interrupt(self):
         self._L.cp_request_interrupt(self._h)
+
+    _CHUNK_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64)
+
+    def set_chunk_callback(self, fn):
+        """fn(evaluated, waiting) after every chunk of a host-driven refinement
+        (cp_set_chunk_callback); fn may call interrupt().  None removes it."""
+        if fn is None:
+            self._chunk_cb = None
+            self._L.cp_set_chunk_callback(self._h, None, None)
+            return
+        self._chunk_cb = self._CHUNK_CB(lambda _u, e, w: fn(int(e), int(w)))
+        self._L.cp_set_chunk_callback(self._h, ctypes.cast(self._chunk_cb, ctypes.c_void_p), None)
 
     @staticmethod
     def opts(family, precision=FP64, policy=SPLIT_UNIFORM, max_depth=2, seed_sizes=None, seed_lambda=None,
@@ -386,6 +428,39 @@ class Prover:
         _check(self._L.cp_random_boxes(self._h, family, seed, max_label, n, _ptr(lo), _ptr(hi), _ptr(dp)),
                "cp_random_boxes")
         return lo, hi, dp
+
+    def proof_defaults(self, family) -> dict:
+        """The library's settings for a family's full-domain proof (cp_proof_defaults)."""
+        o = ProofOpts()
+        _check(self._L.cp_proof_defaults(family, ctypes.byref(o)), "cp_proof_defaults")
+        return o.as_dict()
+
+    def prove_family(self, family, **overrides) -> dict:
+        """The full-domain proof of a family (cp_prove_family): the library's
+        defaults for the family, with any field of cp_proof_opts overridden.
+        An interrupted proof (interrupt()) returns with interrupted=True."""
+        o = ProofOpts()
+        _check(self._L.cp_proof_defaults(family, ctypes.byref(o)), "cp_proof_defaults")
+        for k, v in overrides.items():
+            if k == "seed_sizes":
+                ss = list(v) + [1] * 4
+                for d in range(4):
+                    o.seed_sizes[d] = ss[d]
+            else:
+                setattr(o, k, int(v))
+        r = ProofReport()
+        st = self._L.cp_prove_family(self._h, ctypes.byref(o), ctypes.byref(r))
+        if st not in (0, 8):
+            raise ProverError(st, "cp_prove_family")
+        d = r.as_dict()
+        d["interrupted"] = st == 8
+        return d
+
+    def prove_all(self, precision=FP64, engine=ENGINE_GRAPH) -> list:
+        """The full-domain proofs of the six families in the reference's order (cp_prove_all)."""
+        reps = (ProofReport * 6)()
+        _check(self._L.cp_prove_all(self._h, precision, engine, reps), "cp_prove_all")
+        return [r.as_dict() for r in reps]
 
     def refine_resume(self) -> dict:
         """Continues the refinement interrupted by interrupt() (or loaded from a checkpoint)."""

@@ -322,6 +322,9 @@ struct cp_prover {
     // called before every lattice launch of cp_prove_family_reference
     cp_step_callback step_cb = nullptr;
     void* step_user = nullptr;
+    // called after every chunk of a host-driven refinement
+    cp_chunk_callback chunk_cb = nullptr;
+    void* chunk_user = nullptr;
 };
 
 cudaStream_t cp_prover_stream(cp_prover* p) { return p->stream; }
@@ -565,6 +568,12 @@ cp_status refine_levels(cp_prover* p, const cp_refine_opts& o, cp_refine_report*
         CP_TRY(cp_engine_eval_chunk(p, fam, o, in, begin, c, out, axis, order, &ms));
         ++launches;
         in.n -= c;
+        if (p->chunk_cb) {
+            int64_t evaluated = 0, waiting = 0;
+            for (int v = 0; v < 5; ++v) evaluated += (int64_t)p->h_cnt[C_VERDICT + v];
+            for (const auto& L : p->levels) waiting += (int64_t)L.n;
+            p->chunk_cb(p->chunk_user, evaluated, waiting);
+        }
         if (p->interrupt.load()) {
             p->interrupt.store(0);
             p->pending = true;
@@ -732,6 +741,15 @@ cp_status run_refinement(cp_prover* p, const cp_refine_opts& o, cp_refine_report
     return refine_levels(p, o, r, t0);
 }
 
+// lower end of seed slab k of a proof (slab k covers [cut(k), cut(k + 1)])
+double proof_slab_cut(const cp_proof_opts& o, int k) {
+    if (k <= 0) return kLambdaMin;
+    if (k >= o.slabs) return kLambdaMax;
+    if (!o.geometric) return kLambdaMin + (kLambdaMax - kLambdaMin) / o.slabs * k;
+    // 1 - lambda from 0.5 down to 0.01 by a constant factor per slab
+    return 1.0 - (1.0 - kLambdaMin) * std::pow((1.0 - kLambdaMax) / (1.0 - kLambdaMin), (double)k / o.slabs);
+}
+
 cp_status check_opts(const cp_refine_opts* o) {
     if (!o || o->family < 0 || o->family > 5) return CP_ERR_INVALID;
     if (o->precision != CP_FP64 && o->precision != CP_FP32_PREFILTER) return CP_ERR_INVALID;
@@ -746,6 +764,12 @@ cp_status check_opts(const cp_refine_opts* o) {
 }
 
 }  // namespace
+
+// cp_refine without clearing a pending interrupt request (internal: not exported)
+extern "C" __attribute__((visibility("hidden"))) cp_status cp_refine_keep_interrupt(cp_prover* p,
+                                                                                      const cp_refine_opts* o,
+                                                                                      cp_refine_report* r);
+
 
 extern "C" {
 
@@ -813,6 +837,12 @@ void cp_request_interrupt(cp_prover* p) {
     if (p) p->interrupt.store(1);
 }
 
+void cp_set_chunk_callback(cp_prover* p, cp_chunk_callback cb, void* user) {
+    if (!p) return;
+    p->chunk_cb = cb;
+    p->chunk_user = user;
+}
+
 void cp_set_step_callback(cp_prover* p, cp_step_callback cb, void* user) {
     if (!p) return;
     p->step_cb = cb;
@@ -822,8 +852,15 @@ void cp_set_step_callback(cp_prover* p, cp_step_callback cb, void* user) {
 cp_status cp_refine(cp_prover* p, const cp_refine_opts* o, cp_refine_report* r) {
     if (!p || !r) return CP_ERR_INVALID;
     CP_TRY(check_opts(o));
-    p->pending = false;
     p->interrupt.store(0);  // a request made while no refinement ran does not stop this one
+    return cp_refine_keep_interrupt(p, o, r);
+}
+
+// cp_refine without clearing a pending interrupt request (the proof driver's slabs)
+__attribute__((visibility("hidden"))) cp_status cp_refine_keep_interrupt(cp_prover* p, const cp_refine_opts* o, cp_refine_report* r) {
+    if (!p || !r) return CP_ERR_INVALID;
+    CP_TRY(check_opts(o));
+    p->pending = false;
     const double t0 = now_ms();
     std::memset(r, 0, sizeof(*r));
     CP_TRY(cuda_ok(cudaSetDevice(p->device)));
@@ -853,6 +890,92 @@ cp_status cp_refine(cp_prover* p, const cp_refine_opts* o, cp_refine_report* r) 
     p->levels[0].n = total;
     CP_TRY(reset_counters(p));
     return run_refinement(p, *o, r, t0);
+}
+
+cp_status cp_proof_defaults(int family, cp_proof_opts* o) {
+    if (!o || family < 0 || family > 5) return CP_ERR_INVALID;
+    std::memset(o, 0, sizeof(*o));
+    o->family = family;
+    o->precision = CP_FP64;
+    o->engine = CP_ENGINE_GRAPH;
+    o->policy = CP_SPLIT_LAMBDA;
+    o->max_depth = 24;
+    o->slabs = 1;
+    o->geometric = 0;
+    o->level_capacity = (int64_t)1 << 23;
+    // the radius resolution each family's lambda-only proof needs, with 64
+    // lambda cells over the whole range; start: geometric lambda slabs with the
+    // reference's own radius lattice per slab (start_configuration.cu:41-44)
+    static const int32_t seeds[6][4] = {{1, 256, 256, 64}, {64, 32, 32, 1},  {64, 64, 64, 16},
+                                        {64, 32, 32, 8},   {64, 128, 128, 1}, {64, 32, 32, 8}};
+    for (int d = 0; d < 4; ++d) o->seed_sizes[d] = seeds[family][d];
+    if (family == CP_START) {
+        o->slabs = 18;
+        o->geometric = 1;
+        o->max_depth = 30;
+        o->level_capacity = (int64_t)1 << 24;
+    }
+    return CP_OK;
+}
+
+cp_status cp_prove_family(cp_prover* p, const cp_proof_opts* o, cp_proof_report* r) {
+    if (!p || !o || !r || o->family < 0 || o->family > 5 || o->slabs < 1) return CP_ERR_INVALID;
+    std::memset(r, 0, sizeof(*r));
+    r->first_unresolved_slab = -1;
+    const double t0 = now_ms();
+    p->interrupt.store(0);
+    for (int k = 0; k < o->slabs; ++k) {
+        if (p->interrupt.load()) {
+            p->interrupt.store(0);
+            r->wall_ms = now_ms() - t0;
+            return CP_ERR_INTERRUPTED;
+        }
+        cp_refine_opts ro{};
+        ro.family = o->family;
+        ro.precision = o->precision;
+        ro.policy = o->policy;
+        ro.max_depth = o->max_depth;
+        for (int d = 0; d < 4; ++d) ro.seed_sizes[d] = o->seed_sizes[d] > 0 ? o->seed_sizes[d] : 1;
+        ro.seed_lambda[0] = proof_slab_cut(*o, k);
+        ro.seed_lambda[1] = proof_slab_cut(*o, k + 1);
+        ro.level_capacity = o->level_capacity > 0 ? o->level_capacity : ((int64_t)1 << 24);
+        ro.engine = o->engine;
+        ro.digest = o->digest;
+        ro.seed_parts = o->seed_parts;
+        ro.seed_part = o->seed_part;
+        cp_refine_report rr;
+        const cp_status s = cp_refine_keep_interrupt(p, &ro, &rr);
+        if (s != CP_OK) {
+            r->wall_ms = now_ms() - t0;
+            return s;
+        }
+        r->slabs_done = k + 1;
+        r->evaluated += rr.evaluated;
+        for (int v = 0; v < 5; ++v) r->verdicts[v] += rr.verdicts[v];
+        r->unresolved += rr.unresolved;
+        r->clipped += rr.clipped;
+        for (int d = 0; d < 64; ++d) r->per_depth[d] += rr.per_depth[d];
+        if (rr.max_depth_seen > r->max_depth_seen) r->max_depth_seen = rr.max_depth_seen;
+        if (rr.unresolved && r->first_unresolved_slab < 0) r->first_unresolved_slab = k;
+        r->device_ms += rr.device_ms;
+        r->digest[0] += rr.digest[0];
+        r->digest[1] ^= rr.digest[1];
+    }
+    r->proved = r->unresolved == 0 ? 1 : 0;
+    r->wall_ms = now_ms() - t0;
+    return CP_OK;
+}
+
+cp_status cp_prove_all(cp_prover* p, int precision, int engine, cp_proof_report* reports) {
+    if (!p || !reports) return CP_ERR_INVALID;
+    for (int f = 0; f < 6; ++f) {
+        cp_proof_opts o;
+        CP_TRY(cp_proof_defaults(f, &o));
+        o.precision = precision;
+        o.engine = engine;
+        CP_TRY(cp_prove_family(p, &o, &reports[f]));
+    }
+    return CP_OK;
 }
 
 cp_status cp_random_boxes(cp_prover* p, int family, uint64_t seed, int max_label, size_t n, double* lo, double* hi,

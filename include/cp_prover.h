@@ -167,6 +167,14 @@ void cp_request_interrupt(cp_prover* p);
 typedef void (*cp_step_callback)(void* user, double la_lb, double la_ub);
 void cp_set_step_callback(cp_prover* p, cp_step_callback cb, void* user);
 
+/* Called by the host-driven refinement (CP_ENGINE_LEVELS) after each chunk with
+ * the boxes evaluated so far and the boxes still waiting on all levels: progress
+ * reporting for long refinements.  The callback may call cp_request_interrupt,
+ * which stops the refinement after this chunk (CP_ERR_INTERRUPTED, resumable).
+ * cb = NULL removes it. */
+typedef void (*cp_chunk_callback)(void* user, int64_t evaluated, int64_t waiting);
+void cp_set_chunk_callback(cp_prover* p, cp_chunk_callback cb, void* user);
+
 /* Split policies for the box refinement. */
 typedef enum cp_split_policy {
     CP_SPLIT_UNIFORM = 0, /* bisect every axis (2^dims children) */
@@ -237,6 +245,61 @@ cp_status cp_refine(cp_prover* p, const cp_refine_opts* opts, cp_refine_report* 
  * may be NULL = 0). */
 cp_status cp_refine_boxes(cp_prover* p, const cp_refine_opts* opts, const double* lo, const double* hi,
                           const uint8_t* depth, size_t n, cp_refine_report* report);
+
+/* ---------------------------------------------------------------- full-domain proofs
+ * The proof of a family over its whole domain (lambda in [0.5, 0.99] and the
+ * dependent radius ranges) by the box refinement: the lambda range is cut into
+ * seed slabs, each slab is seeded with a lattice (seed_sizes subdivisions of
+ * lambda, r1, r2[, r3] over the slab's own dependent ranges, like the
+ * reference's lattices) and refined with `policy` (default lambda only, the
+ * reference's own refinement rule, run_kernel.cuh:110-127) down to max_depth.
+ * The family is proved when no box is left unresolved.  Stands beside the
+ * reference's find_critical_intervals_*_configuration() drivers
+ * (lane_packing.cu:27-37) for callers that want the adaptive engine. */
+typedef struct cp_proof_opts {
+    int32_t family;
+    int32_t precision;       /* cp_precision */
+    int32_t engine;          /* cp_engine */
+    int32_t policy;          /* cp_split_policy (CP_SPLIT_LAMBDA recommended) */
+    int32_t max_depth;       /* <= 250 */
+    int32_t slabs;           /* seed lambda slabs (>= 1) */
+    int32_t geometric;       /* 1: 1 - lambda shrinks by a constant factor from slab to slab
+                                (narrower slabs toward 0.99, where the needed lambda width shrinks);
+                                0: equal widths */
+    int32_t seed_sizes[4];   /* lattice subdivisions per slab: lambda, r1, r2[, r3] */
+    int64_t level_capacity;  /* 0 = 1 << 24 */
+    int32_t digest;          /* 1 = per-box verdict digest in the report */
+    int32_t seed_parts;      /* > 1: refine only the interleaved piece seed_part of every slab's lattice */
+    int32_t seed_part;       /* (one rank's share of the proof, see cp_refine_opts) */
+} cp_proof_opts;
+
+typedef struct cp_proof_report {
+    int32_t proved;           /* 1: every slab refined with no unresolved box */
+    int32_t slabs_done;
+    int64_t evaluated;
+    int64_t verdicts[5];
+    int64_t unresolved;
+    int64_t clipped;
+    int64_t per_depth[64];
+    int32_t max_depth_seen;
+    int32_t first_unresolved_slab; /* -1 when none */
+    double device_ms, wall_ms;
+    uint64_t digest[2];
+} cp_proof_report;
+
+/* The library's settings for a family's full-domain proof (the seeds its
+ * refinement needs); CP_ERR_INVALID for a bad family. */
+cp_status cp_proof_defaults(int family, cp_proof_opts* opts);
+
+/* The proof of one family (opts->family).  Stops between slabs on
+ * cp_request_interrupt (CP_ERR_INTERRUPTED, report->slabs_done).  Returns CP_OK
+ * when the refinement ran to completion; report->proved tells the outcome. */
+cp_status cp_prove_family(cp_prover* p, const cp_proof_opts* opts, cp_proof_report* report);
+
+/* The proofs of all six families in the reference's order (lane_packing.cu:32-37),
+ * each with cp_proof_defaults and the given precision and engine; reports:
+ * 6 entries.  Returns the first error status, CP_OK otherwise. */
+cp_status cp_prove_all(cp_prover* p, int precision, int engine, cp_proof_report* reports);
 
 /* ---------------------------------------------------------------- reference semantics
  * One launch of a family kernel over one lambda interval with the reference's

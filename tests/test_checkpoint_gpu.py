@@ -18,20 +18,36 @@ def test_interrupt_resume_and_checkpoint(cp, tmp_path, family, policy):
     try:
         want = p.refine(family, **kw)
         assert want["launches"] > 2  # several chunks, so an interrupt lands between them
-        # same handle: interrupt after the first chunk, then resume
+        # an interrupt requested while no refinement runs does not stop the next one
         p.interrupt()
+        again = p.refine(family, **kw)
+        for k in KEYS:
+            assert again[k] == want[k], k
+        # same handle: interrupt after the first chunk (from the progress callback), then resume
+        seen = []
+
+        def stop_after_first(evaluated, waiting):
+            if not seen:
+                p.interrupt()
+            seen.append((evaluated, waiting))
+
+        p.set_chunk_callback(stop_after_first)
         with pytest.raises(cp.ProverError) as e:
             p.refine(family, **kw)
         assert e.value.status == 8  # CP_ERR_INTERRUPTED
+        assert len(seen) == 1 and 0 < seen[0][0] < want["evaluated"]
+        p.set_chunk_callback(None)
         got = p.refine_resume()
         for k in KEYS:
             assert got[k] == want[k], k
         with pytest.raises(cp.ProverError):
             p.refine_resume()  # nothing left to resume
         # checkpoint: interrupt, save, continue in a new handle
-        p.interrupt()
+        seen.clear()
+        p.set_chunk_callback(stop_after_first)
         with pytest.raises(cp.ProverError):
             p.refine(family, **kw)
+        p.set_chunk_callback(None)
         path = tmp_path / "refine.ckpt"
         p.checkpoint_save(str(path))
     finally:
