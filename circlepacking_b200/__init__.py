@@ -300,6 +300,18 @@ def div_check(a, b):
     return out.cpu().numpy().T
 
 
+def fdiv_check(a, b):
+    """(library RD, library RU, __fdiv_rd, __fdiv_ru) of float32 a/b on the device, as numpy arrays."""
+    torch = _torch()
+    L = lib()
+    L.cp_fdiv_check.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]
+    a = _dev(np.asarray(a, np.float32), torch.float32)
+    b = _dev(np.asarray(b, np.float32), torch.float32)
+    out = torch.empty((a.numel(), 4), dtype=torch.float32, device="cuda")
+    _check(L.cp_fdiv_check(_ptr(a), _ptr(b), a.numel(), _ptr(out), _stream()), "cp_fdiv_check")
+    return out.cpu().numpy().T
+
+
 def _sizes4(sizes):
     if sizes is None:
         return None

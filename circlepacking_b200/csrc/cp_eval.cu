@@ -68,6 +68,18 @@ __global__ void __launch_bounds__(kEvalBlock) k_eval_prefilter(const double* __r
     }
 }
 
+// The FP32 pre-pass's directed division against the CUDA intrinsics it replaces.
+__global__ void k_fdiv_check(const float* __restrict__ a, const float* __restrict__ b, size_t n,
+                             float* __restrict__ out) {
+    const size_t step = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step) {
+        out[4 * i + 0] = f32::fdiv_rd(a[i], b[i]);
+        out[4 * i + 1] = f32::fdiv_ru(a[i], b[i]);
+        out[4 * i + 2] = __fdiv_rd(a[i], b[i]);
+        out[4 * i + 3] = __fdiv_ru(a[i], b[i]);
+    }
+}
+
 // The library's directed division against the CUDA intrinsics it replaces.
 __global__ void k_div_check(const double* __restrict__ a, const double* __restrict__ b, size_t n,
                             double* __restrict__ out) {
@@ -318,6 +330,13 @@ cp_status cp_div_check(const double* a, const double* b, size_t n, double* out, 
     if (n == 0) return CP_OK;
     if (!a || !b || !out) return CP_ERR_INVALID;
     k_div_check<<<grid_for(k_div_check, n, 128), 128, 0, (cudaStream_t)stream>>>(a, b, n, out);
+    return cp_check_launch();
+}
+
+cp_status cp_fdiv_check(const float* a, const float* b, size_t n, float* out, void* stream) {
+    if (n == 0) return CP_OK;
+    if (!a || !b || !out) return CP_ERR_INVALID;
+    k_fdiv_check<<<grid_for(k_fdiv_check, n, 128), 128, 0, (cudaStream_t)stream>>>(a, b, n, out);
     return cp_check_launch();
 }
 

@@ -45,17 +45,54 @@ __device__ __forceinline__ E emul(E a, E b) {
     const float q1 = __fmul_ru(a.l, b.l), q2 = __fmul_ru(a.l, b.u), q3 = __fmul_ru(a.u, b.l), q4 = __fmul_ru(a.u, b.u);
     return {fminf(fminf(p1, p2), fminf(p3, p4)), fmaxf(fmaxf(q1, q2), fmaxf(q3, q4))};
 }
+// a / b rounded down (UP = false) or up, bit-identical to __fdiv_rd / __fdiv_ru.
+// For |a|, |b| in [2^-60, 2^61): y = rcp.approx(b) (relative error ~2^-23),
+// q0 = a*y, then one correction q = q0 + (a - q0*b)*y leaves |q - a/b| far
+// below an ulp of q plus half an ulp, so q is faithful; the remainder
+// r = a - q*b (one FMA) is then nonzero exactly when a/b != q and keeps its
+// sign (|r| >= 2^-107, no underflow), which picks the directed result among q
+// and its neighbour.  Other operands (zeros, subnormals, large exponents,
+// infinities, NaN) use the IEEE intrinsics.  One shared (not inlined) copy per
+// direction keeps the level kernels within the instruction caches.
+__device__ __forceinline__ bool fdiv_in_range(float a, float b) {
+    const unsigned ea = (__float_as_uint(a) >> 23) & 0xffu, eb = (__float_as_uint(b) >> 23) & 0xffu;
+    return (ea - 67u) <= 120u && (eb - 67u) <= 120u;
+}
+__device__ __forceinline__ float fnext_up(float q) {  // q finite, normal, nonzero
+    const int b = __float_as_int(q);
+    return __int_as_float(q > 0.f ? b + 1 : b - 1);
+}
+__device__ __forceinline__ float fnext_down(float q) {
+    const int b = __float_as_int(q);
+    return __int_as_float(q > 0.f ? b - 1 : b + 1);
+}
+template <bool UP>
+__device__ __forceinline__ float fdiv_dir_inline(float a, float b) {
+    if (!fdiv_in_range(a, b)) return UP ? __fdiv_ru(a, b) : __fdiv_rd(a, b);
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
+    float q = __fmul_rn(a, y);
+    q = __fmaf_rn(__fmaf_rn(-q, b, a), y, q);
+    const float r = __fmaf_rn(-q, b, a);
+    if (r == 0.f) return q;
+    const bool above = (r > 0.f) != (b < 0.f);  // a/b > q
+    if (UP) return above ? fnext_up(q) : q;
+    return above ? q : fnext_down(q);
+}
+static __device__ __noinline__ float fdiv_rd(float a, float b) { return fdiv_dir_inline<false>(a, b); }
+static __device__ __noinline__ float fdiv_ru(float a, float b) { return fdiv_dir_inline<true>(a, b); }
+
 // enclosure of a/b; the divisor enclosure must exclude 0
 __device__ __forceinline__ E ediv(E a, E b, bool& ok) {
     if (b.l > 0.f) {
-        if (a.l >= 0.f) return {__fdiv_rd(a.l, b.u), __fdiv_ru(a.u, b.l)};
-        if (a.u <= 0.f) return {__fdiv_rd(a.l, b.l), __fdiv_ru(a.u, b.u)};
-        return {__fdiv_rd(a.l, b.l), __fdiv_ru(a.u, b.l)};
+        if (a.l >= 0.f) return {fdiv_rd(a.l, b.u), fdiv_ru(a.u, b.l)};
+        if (a.u <= 0.f) return {fdiv_rd(a.l, b.l), fdiv_ru(a.u, b.u)};
+        return {fdiv_rd(a.l, b.l), fdiv_ru(a.u, b.l)};
     }
     if (b.u < 0.f) {
-        if (a.l >= 0.f) return {__fdiv_rd(a.u, b.u), __fdiv_ru(a.l, b.l)};
-        if (a.u <= 0.f) return {__fdiv_rd(a.u, b.l), __fdiv_ru(a.l, b.u)};
-        return {__fdiv_rd(a.u, b.u), __fdiv_ru(a.l, b.u)};
+        if (a.l >= 0.f) return {fdiv_rd(a.u, b.u), fdiv_ru(a.l, b.l)};
+        if (a.u <= 0.f) return {fdiv_rd(a.u, b.l), fdiv_ru(a.l, b.u)};
+        return {fdiv_rd(a.u, b.u), fdiv_ru(a.l, b.u)};
     }
     ok = false;
     return {-INFINITY, INFINITY};
@@ -87,6 +124,11 @@ __device__ __forceinline__ float fstep_down(float y, int n) {
 }
 __device__ __forceinline__ float fstep_up(float y, int n) { return -fstep_down(-y, n); }
 
+// asinf padded kAsinfSteps single steps down / up: one shared (not inlined)
+// copy each, like the FP64 asin, for the instruction caches
+static __device__ __noinline__ float asinf_down(float x) { return fstep_down(asinf(x), kAsinfSteps); }
+static __device__ __noinline__ float asinf_up(float x) { return fstep_up(asinf(x), kAsinfSteps); }
+
 // enclosure of asin_rd64(v) and asin_ru64(v) for every FP64 v in x
 __device__ __forceinline__ E easin(E x, bool& ok) {
     if (!(x.l >= -1.f && x.u <= 1.f)) {
@@ -94,8 +136,8 @@ __device__ __forceinline__ E easin(E x, bool& ok) {
         return {-2.f, 2.f};
     }
     const float pi2 = 1.57079637f;  // >= 1.5707963267948968 (interval.cuh:366)
-    float lo = fstep_down(asinf(x.l), kAsinfSteps);
-    float hi = fstep_up(asinf(x.u), kAsinfSteps);
+    float lo = asinf_down(x.l);
+    float hi = asinf_up(x.u);
     if (lo < -pi2) lo = -pi2;
     if (x.l >= 0.f && lo < 0.f) lo = 0.f;
     if (hi > pi2) hi = pi2;
@@ -111,7 +153,11 @@ __device__ __forceinline__ EI ei(double lo, double hi) { return {ec(lo), ec(hi)}
 __device__ __forceinline__ EI ept(E x) { return {x, x}; }
 __device__ __forceinline__ EI iadd(EI a, EI b) { return {eadd(a.lo, b.lo), eadd(a.hi, b.hi)}; }
 __device__ __forceinline__ EI isub(EI a, EI b) { return {esub(a.lo, b.hi), esub(a.hi, b.lo)}; }
-__device__ __forceinline__ EI iscale(float n, EI a) { return {emul(a.lo, ek(n)), emul(a.hi, ek(n))}; }
+// scaling by a positive constant is monotone: round the lower ends down and the
+// upper ends up (exact for the powers of two used here, except near underflow)
+__device__ __forceinline__ EI iscale(float n, EI a) {
+    return {{__fmul_rd(a.lo.l, n), __fmul_ru(a.lo.u, n)}, {__fmul_rd(a.hi.l, n), __fmul_ru(a.hi.u, n)}};
+}
 // Three-valued comparison outcome of enclosed FP64 values.  Branches that only
 // select between two values take the hull of both candidates when undecided.
 enum Tri { T_FALSE = 0, T_TRUE = 1, T_UNKNOWN = 2 };
@@ -180,7 +226,7 @@ __device__ __forceinline__ void tight_hi(EI& a, E x, bool&) { a.hi = emin(a.hi, 
 
 // shadow of collision<W> (cp_fp64.cuh); trap events clear ok
 template <int W>
-__device__ __noinline__ E collision(EI L, EI S, EI ab, bool& ok) {
+__device__ __forceinline__ E collision_body(EI L, EI S, EI ab, bool& ok) {
     constexpr bool HI = (W == W_HI);
     L.lo = emax(L.lo, S.lo);
     S.hi = emin(S.hi, L.hi);
@@ -289,6 +335,26 @@ __device__ __noinline__ E collision(EI L, EI S, EI ab, bool& ok) {
     return ob_val;
 }
 
+// One shared (not inlined) copy per Want, with the certification flag in a
+// register of its own: a flag passed by reference into an out-of-line function
+// lives in local memory, and the shadow reads it after almost every step.
+struct EOk {
+    E v;
+    bool ok;
+};
+template <int W>
+__device__ __noinline__ EOk collision_call(EI L, EI S, EI ab) {
+    bool ok = true;
+    const E v = collision_body<W>(L, S, ab, ok);
+    return {v, ok};
+}
+template <int W>
+__device__ __forceinline__ E collision(EI L, EI S, EI ab, bool& ok) {
+    const EOk r = collision_call<W>(L, S, ab);
+    ok = ok && r.ok;
+    return r.v;
+}
+
 // corner wrappers (shadows of cp_fp64.cuh); LOC = lower-bound corner, which
 // returns 0 when the radii sum is not positive (collision_angles.cu:131-137, 222-228)
 // ra, rb: the exact FP64 corner radii; ra >= rb makes the corner intervals
@@ -381,7 +447,7 @@ __device__ __forceinline__ bool holds(E lhs, E rhs, bool& ok) { return !clt(lhs,
 
 // ---------------------------------------------------------------- families
 // handle_case_1_1 / handle_case_2_1 (middle_configuration.cu:86-154); true = failed
-__device__ __forceinline__ bool middle_handle(const BI& Bla, const BI& Br1, const BI& Br2, const BI& Br3, bool inner_first,
+__device__ __forceinline__ bool middle_handle_body(const BI& Bla, const BI& Br1, const BI& Br2, const BI& Br3, bool inner_first,
                                              bool& ok, int* sub) {
     const EI la = Bla.e, r1 = Br1.e, r2 = Br2.e, r3 = Br3.e;
     const E ratio = area_ratio_ub(la);
@@ -429,7 +495,7 @@ __device__ __forceinline__ bool middle_handle(const BI& Bla, const BI& Br1, cons
 }
 
 template <bool INNER>
-__device__ __forceinline__ bool end2d_handle(EI la, EI r1, EI r2, bool& ok) {
+__device__ __forceinline__ bool end2d_handle_body(EI la, EI r1, EI r2, bool& ok) {
     EI ca, sa;
     E other_hi, rho_lo;
     if (INNER) {
@@ -455,7 +521,7 @@ __device__ __forceinline__ bool end2d_handle(EI la, EI r1, EI r2, bool& ok) {
 }
 
 template <bool INNER>
-__device__ __forceinline__ bool end3d_handle(const BI& Bla, const BI& Br1, const BI& Br2, const BI& Br3, bool& ok) {
+__device__ __forceinline__ bool end3d_handle_body(const BI& Bla, const BI& Br1, const BI& Br2, const BI& Br3, bool& ok) {
     const EI la = Bla.e, r1 = Br1.e, r2 = Br2.e, r3 = Br3.e;
     E a12_lo, a23_lo, a13_hi;
     if (INNER) {
@@ -504,6 +570,28 @@ __device__ __forceinline__ bool end3d_handle(const BI& Bla, const BI& Br1, const
     const E lhs = eadd(eadd(disk_area_lb(r2), disk_area_lb(r3)), emul(ek(0.5f), disk_area_lb(r1)));
     const E rhs = emul(kcr(), esub(used, reusable));
     return !holds(lhs, rhs, ok);
+}
+
+// Out-of-line handles (one copy each) taking their boxes by value and returning
+// a packed status, so no flag or box lives in local memory: -2 = not certified,
+// -1 = the handle holds, k >= 0 = sub-check k fails.
+static __device__ __noinline__ int middle_handle_call(BI Bla, BI Br1, BI Br2, BI Br3, bool inner_first) {
+    bool ok = true;
+    int sub = 0;
+    const bool failed = middle_handle_body(Bla, Br1, Br2, Br3, inner_first, ok, &sub);
+    return !ok ? -2 : failed ? sub : -1;
+}
+template <bool INNER>
+__device__ __noinline__ int end2d_handle_call(EI la, EI r1, EI r2) {
+    bool ok = true;
+    const bool failed = end2d_handle_body<INNER>(la, r1, r2, ok);
+    return !ok ? -2 : failed ? 0 : -1;
+}
+template <bool INNER>
+__device__ __noinline__ int end3d_handle_call(BI Bla, BI Br1, BI Br2, BI Br3) {
+    bool ok = true;
+    const bool failed = end3d_handle_body<INNER>(Bla, Br1, Br2, Br3, ok);
+    return !ok ? -2 : failed ? 0 : -1;
 }
 
 }  // namespace f32
@@ -594,20 +682,30 @@ __device__ __forceinline__ int prefilter_box(const double* lo, const double* hi,
         const bool second_first = (order & 1) != 0;
         for (int h = 0; h < 2 && ok && fail_bit < 0; ++h) {
             const bool inner = (h == 0) != second_first;
-            int sub = 0;
-            if (middle_handle(Bla, Br1, Br2, Br3, inner, ok, &sub)) fail_bit = (inner ? 0 : 2) + sub;
+            const int r = middle_handle_call(Bla, Br1, Br2, Br3, inner);
+            if (r == -2)
+                ok = false;
+            else if (r >= 0)
+                fail_bit = (inner ? 0 : 2) + r;
         }
     } else if (FAM == F_END_2D) {
         const bool second_first = (order & 1) != 0;
         for (int h = 0; h < 2 && ok && fail_bit < 0; ++h) {
             const bool inner = (h == 0) != second_first;
-            if (inner ? end2d_handle<true>(la, r1, r2, ok) : end2d_handle<false>(la, r1, r2, ok)) fail_bit = inner ? 0 : 1;
+            const int r = inner ? end2d_handle_call<true>(la, r1, r2) : end2d_handle_call<false>(la, r1, r2);
+            if (r == -2)
+                ok = false;
+            else if (r >= 0)
+                fail_bit = inner ? 0 : 1;
         }
     } else if (FAM == F_END_3D) {
         const bool second_first = (order & 1) != 0;
         for (int h = 0; h < 2 && ok && fail_bit < 0; ++h) {
             const bool inner = (h == 0) != second_first;
-            if (inner ? end3d_handle<true>(Bla, Br1, Br2, Br3, ok) : end3d_handle<false>(Bla, Br1, Br2, Br3, ok))
+            const int r = inner ? end3d_handle_call<true>(Bla, Br1, Br2, Br3) : end3d_handle_call<false>(Bla, Br1, Br2, Br3);
+            if (r == -2)
+                ok = false;
+            else if (r >= 0)
                 fail_bit = inner ? 0 : 1;
         }
     }

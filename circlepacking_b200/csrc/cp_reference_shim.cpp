@@ -47,6 +47,17 @@ void on_sigint(int) {
     if (g_active) cp_request_interrupt(g_active);
 }
 
+// The reference installs its handler when a family's lambda loop starts
+// (run_kernel.cuh:51-54, after the banner) and checks the flag after every
+// launch.  Here the handler is installed just before the banner, and a signal
+// that came before the loop started is handed to it before the first launch
+// (on_step), so it takes effect after that launch as in the reference.
+void arm() {
+    g_interrupts = 0;
+    g_previous = std::signal(SIGINT, on_sigint);
+}
+void disarm() { std::signal(SIGINT, g_previous); }
+
 cp_prover* handle() {
     static cp_prover* h = nullptr;
     if (!h) {
@@ -109,6 +120,7 @@ void print_criticals(cp_prover* p, int family, double lb, double ub) {
 // operator<< writes it (interval.hpp:295-303): right-aligned fields of width 26,
 // 19 significant digits.
 void on_step(void*, double lb, double ub) {
+    if (g_interrupts && g_active) cp_request_interrupt(g_active);
     const std::ios_base::fmtflags flags = std::cerr.flags(std::ios::right);
     const std::streamsize prec = std::cerr.precision(19);
     std::cerr << "Handling lambda interval " << '[' << std::setw(26) << lb << ", " << std::setw(26) << ub << ']'
@@ -120,13 +132,10 @@ void on_step(void*, double lb, double ub) {
 // run_kernel_until_no_criticals for one family; true when the lambda queue emptied
 bool run_family(int family) {
     cp_prover* p = handle();
-    g_interrupts = 0;
     g_active = p;
-    g_previous = std::signal(SIGINT, on_sigint);
     cp_set_step_callback(p, on_step, nullptr);
     cp_reference_report r;
     const cp_status s = cp_prove_family_reference(p, family, kLambdaMin, kLambdaMax, nullptr, 0, nullptr, &r);
-    std::signal(SIGINT, g_previous);
     cp_set_step_callback(p, nullptr, nullptr);
     g_active = nullptr;
     if (s == CP_ERR_INTERRUPTED) {
@@ -149,27 +158,39 @@ namespace circlepacking {
 namespace lane_packing {
 
 void find_critical_intervals_start_configuration() {
+    arm();
     std::cout << "Start configuration..." << std::endl;
     run_family(CP_START);
+    disarm();
 }
 
 void find_critical_intervals_start_end_configuration() {
+    arm();
     std::cout << "Start & end configuration, 2 disks... " << std::endl;
     run_family(CP_START_END_2D);
+    disarm();
+    arm();
     std::cerr << "Start & end configuration, 3 disks ..." << std::endl;
     run_family(CP_START_END_3D);
+    disarm();
 }
 
 void find_critical_intervals_middle_configuration() {
+    arm();
     std::cout << "Middle configuration ..." << std::endl;
     run_family(CP_MIDDLE);
+    disarm();
 }
 
 void find_critical_intervals_end_configuration() {
+    arm();
     std::cout << "End configuration (2 disks) ..." << std::endl;
     run_family(CP_END_2D);
+    disarm();
+    arm();
     std::cout << "End configuration (3 disks) ..." << std::endl;
     run_family(CP_END_3D);
+    disarm();
 }
 
 void find_critical_intervals() {

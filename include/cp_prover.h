@@ -362,6 +362,12 @@ cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* opts, const d
  * (library RD, library RU, __ddiv_rd, __ddiv_ru).  Asynchronous. */
 cp_status cp_div_check(const double* a, const double* b, size_t n, double* out, void* stream);
 
+/* Diagnostics: the FP32 pre-pass's directed division (Newton-corrected
+ * reciprocal quotient and exact FMA remainder sign) next to the IEEE intrinsics
+ * __fdiv_rd / __fdiv_ru it replaces.  a, b: n device floats; out: 4n device
+ * floats per element (library RD, library RU, __fdiv_rd, __fdiv_ru). */
+cp_status cp_fdiv_check(const float* a, const float* b, size_t n, float* out, void* stream);
+
 /* Diagnostics: measured peak throughput (operations per second, whole device)
  * of the FP64 primitives the criteria use, each run alone with full occupancy
  * and independent chains: rates[0] DFMA, [1] __dadd_rd, [2] __dmul_rd,

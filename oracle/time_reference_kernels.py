@@ -26,7 +26,9 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-sys.path.insert(0, ROOT)
+# run as a script, this file's own directory comes first on the path, where
+# `oracle` would name oracle/oracle.py instead of the package
+sys.path[:] = [ROOT] + [p for p in sys.path if os.path.abspath(p or ".") != os.path.dirname(os.path.abspath(__file__))]
 
 LAMBDA = (0.5, 0.9900000000000001)  # values.hpp:31-32
 DBL_MAX = np.finfo(np.float64).max

@@ -1,11 +1,14 @@
 """The drop-in driver on a B200: the reference's prover.cpp, linked unchanged
 against the library's C++ shim, runs the six families in the reference's order
 (lane_packing.cu:32-37).  The test interrupts every family once with SIGINT
-after its first "Handling lambda interval" line (run_kernel.cuh:79) and checks
-what the reference's SIGINT path prints (run_kernel.cuh:86-108): the
-"We were interrupted" line, then the failing boxes of the first remaining lambda
-interval in the family's own line format (e.g. middle_configuration.cu:182,
-end_configuration.cu:124, start_configuration.cu:289).
+when its banner appears, so the interrupt takes effect after the family's
+first launch over the whole lambda range (which holds failing boxes for every
+family), and checks what the reference's SIGINT path prints
+(run_kernel.cuh:86-108): the "We were interrupted" line, then the failing
+boxes of that interval in the family's own line format (e.g.
+middle_configuration.cu:182, end_configuration.cu:124,
+start_configuration.cu:289).  Every launch is announced on stderr as
+"Handling lambda interval [lb, ub]" (run_kernel.cuh:79).
 
 When the reference-linked binary (oracle/_ref/prover_b200, built by
 `make -C oracle ref`) is absent, the test builds the same three-line main from
@@ -106,11 +109,10 @@ def test_prover_sigint_prints_reference_format(cp, tmp_path):
                 continue
             lines.append((tag, line))
             for k, (banner, _) in enumerate(FAMILIES):
-                if (tag, line) == banner:
+                if (tag, line) == banner and k not in interrupted:
                     fam = k
-            if tag == "err" and line.startswith("Handling lambda interval") and fam >= 0 and fam not in interrupted:
-                interrupted.add(fam)
-                proc.send_signal(signal.SIGINT)
+                    interrupted.add(k)
+                    proc.send_signal(signal.SIGINT)
         rc = proc.wait(timeout=60)
     finally:
         if proc.poll() is None:
