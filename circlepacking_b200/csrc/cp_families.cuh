@@ -42,8 +42,8 @@ __device__ __forceinline__ void trace_put(double* tr, int k, double lhs, double 
 // handles are not inlined: one copy each keeps the kernels within the
 // instruction caches (measured 6-9% faster on middle and end_3d).
 template <int MODE>
-__device__ __noinline__ bool middle_handle(Iv la, Iv r1, Iv r2, Iv r3, bool inner_first, uint8_t& mask, int k0,
-                                             bool& trap, double* tr) {
+__device__ __forceinline__ bool middle_handle(Iv la, Iv r1, Iv r2, Iv r3, bool inner_first, uint8_t& mask, int k0,
+                                              bool& trap, double* tr) {
     const double ratio = area_ratio_ub(la);
     const double a1 = disk_area_lb(r1), a2 = disk_area_lb(r2);
     // guard "possibly": c13.lo <= (c12 + c23).hi
@@ -96,7 +96,7 @@ __device__ __noinline__ bool middle_handle(Iv la, Iv r1, Iv r2, Iv r3, bool inne
 
 // handle_inner_outer_2d (INNER) / handle_outer_inner_2d, end_configuration.cu:71-101
 template <bool INNER>
-__device__ __noinline__ bool end2d_handle(Iv la, Iv r1, Iv r2, bool& trap, double* lhs_out, double* rhs_out) {
+__device__ __forceinline__ bool end2d_handle(Iv la, Iv r1, Iv r2, bool& trap, double* lhs_out, double* rhs_out) {
     Iv ca, sa;
     double other_hi, rho_lo;
     if (INNER) {
@@ -126,8 +126,8 @@ __device__ __noinline__ bool end2d_handle(Iv la, Iv r1, Iv r2, bool& trap, doubl
 // handle_r1_inner_3d (INNER) / handle_r1_outer_3d, end_configuration.cu:154-210.
 // Returns true when the handle fails; *evaluated = false on the early exit.
 template <bool INNER>
-__device__ __noinline__ bool end3d_handle(Iv la, Iv r1, Iv r2, Iv r3, bool& trap, bool* evaluated, double* lhs_out,
-                                             double* rhs_out) {
+__device__ __forceinline__ bool end3d_handle(Iv la, Iv r1, Iv r2, Iv r3, bool& trap, bool* evaluated, double* lhs_out,
+                                              double* rhs_out) {
     // early exit: definitely(a12 + a23 >= a13)  <=>  a13.hi <= (a12 + a23).lo
     double a12_lo, a23_lo, a13_hi;
     if (INNER) {
@@ -186,6 +186,36 @@ __device__ __noinline__ bool end3d_handle(Iv la, Iv r1, Iv r2, Iv r3, bool& trap
     *lhs_out = __dadd_rd(__dadd_rd(ar2, ar3), __dmul_rd(0.5, ar1));
     *rhs_out = __dmul_ru(kCriticalRatio, __dadd_ru(used, -reusable));
     return !(*lhs_out >= *rhs_out);
+}
+
+// Out-of-line copies of the handles (one each), with every flag and result in
+// registers: the bodies above are inlined into these, and each returns what
+// its caller needs (flags packed, the compared pair for traces) by value.
+struct HandleOut {
+    double lhs, rhs;
+    uint32_t bits;  // bit 0: failed, bit 1: trap site reached, bit 2: criterion evaluated; bits 8..15: mask
+};
+template <int MODE>
+__device__ __noinline__ HandleOut middle_handle_call(Iv la, Iv r1, Iv r2, Iv r3, bool inner_first, int k0,
+                                                     double* tr) {
+    uint8_t mask = 0;
+    bool trap = false;
+    const bool failed = middle_handle<MODE>(la, r1, r2, r3, inner_first, mask, k0, trap, tr);
+    return {0.0, 0.0, (failed ? 1u : 0u) | (trap ? 2u : 0u) | ((uint32_t)mask << 8)};
+}
+template <bool INNER>
+__device__ __noinline__ HandleOut end2d_handle_call(Iv la, Iv r1, Iv r2) {
+    bool trap = false;
+    double lhs = 0.0, rhs = 0.0;
+    const bool failed = end2d_handle<INNER>(la, r1, r2, trap, &lhs, &rhs);
+    return {lhs, rhs, (failed ? 1u : 0u) | (trap ? 2u : 0u) | 4u};
+}
+template <bool INNER>
+__device__ __noinline__ HandleOut end3d_handle_call(Iv la, Iv r1, Iv r2, Iv r3) {
+    bool trap = false, evaluated = false;
+    double lhs = 0.0, rhs = 0.0;
+    const bool failed = end3d_handle<INNER>(la, r1, r2, r3, trap, &evaluated, &lhs, &rhs);
+    return {lhs, rhs, (failed ? 1u : 0u) | (trap ? 2u : 0u) | (evaluated ? 4u : 0u)};
 }
 
 // Evaluates one raw box.  lo/hi hold the family's dims axes (la, r1, r2, r3).
@@ -294,7 +324,10 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
         for (int h = 0; h < 2; ++h) {
             const bool inner = (h == 0) != second_first;
             ++handles;
-            bool failed = middle_handle<MODE>(la, r1, r2, r3, inner, mask, inner ? 0 : 2, trap, tr);
+            const HandleOut o = middle_handle_call<MODE>(la, r1, r2, r3, inner, inner ? 0 : 2, tr);
+            mask |= (uint8_t)(o.bits >> 8);
+            if (o.bits & 2u) trap = true;
+            const bool failed = (o.bits & 1u) != 0;
             if (MODE == DECIDE && failed) break;
         }
     } else if (FAM == F_END_2D) {
@@ -302,8 +335,11 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
         for (int h = 0; h < 2; ++h) {
             const bool inner = (h == 0) != second_first;
             ++handles;
-            bool failed = inner ? end2d_handle<true>(la, r1, r2, trap, &lhs, &rhs)
-                                : end2d_handle<false>(la, r1, r2, trap, &lhs, &rhs);
+            const HandleOut o = inner ? end2d_handle_call<true>(la, r1, r2) : end2d_handle_call<false>(la, r1, r2);
+            lhs = o.lhs;
+            rhs = o.rhs;
+            if (o.bits & 2u) trap = true;
+            const bool failed = (o.bits & 1u) != 0;
             const int k = inner ? 0 : 1;
             if (MODE == FULL) trace_put(tr, k, lhs, rhs);
             if (failed) {
@@ -317,8 +353,13 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
             const bool inner = (h == 0) != second_first;
             ++handles;
             bool evaluated = false;
-            bool failed = inner ? end3d_handle<true>(la, r1, r2, r3, trap, &evaluated, &lhs, &rhs)
-                                : end3d_handle<false>(la, r1, r2, r3, trap, &evaluated, &lhs, &rhs);
+            const HandleOut o =
+                inner ? end3d_handle_call<true>(la, r1, r2, r3) : end3d_handle_call<false>(la, r1, r2, r3);
+            lhs = o.lhs;
+            rhs = o.rhs;
+            evaluated = (o.bits & 4u) != 0;
+            if (o.bits & 2u) trap = true;
+            const bool failed = (o.bits & 1u) != 0;
             const int k = inner ? 0 : 1;
             if (MODE == FULL && evaluated) trace_put(tr, k, lhs, rhs);
             if (failed) {

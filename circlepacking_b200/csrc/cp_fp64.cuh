@@ -187,6 +187,18 @@ __device__ __forceinline__ bool iempty(Iv a) { return a.lo > a.hi; }
 __device__ __forceinline__ double dmax_lo(double a, double b) { return a < b ? b : a; }  // "a < b ? b : a"
 
 // ------------------------------------------------------------------ collision angle
+// x / o takes the positive branches of the interval division (o.lo > 0,
+// x.lo >= 0), both intervals are proper, and the lower-end quotient's operands
+// lie in the certified division's range (so an FMA remainder has an exact sign).
+__device__ __forceinline__ bool posq(Iv x, Iv o) {
+    return o.lo > 0.0 && x.lo >= 0.0 && x.lo <= x.hi && o.lo <= o.hi && div_in_range(x.lo, o.hi);
+}
+// RD(a / b) > 1 for a >= 0, b > 0 in range: a / b >= 1 + 2^-52, i.e. the exact
+// a - b * (1 + 2^-52) is not negative (one FMA; its rounding keeps the sign).
+__device__ __forceinline__ bool rd_quot_gt1(double a, double b) {
+    return __fma_rn(-b, 1.0000000000000002, a) >= 0.0;
+}
+
 // What a caller needs from compute_collision_angle: one bound, or only whether
 // a trap site is reached (for corners the reference evaluates but whose value no
 // criterion consumes; every trap condition is decided before any asin).
@@ -194,7 +206,7 @@ enum Want : int { W_LO = 0, W_HI = 1, W_TRAP = 2 };
 
 // compute_collision_angle (collision_angles.cu:37-117) for one Want.
 template <int W>
-__device__ __noinline__ double collision(Iv L, Iv S, Iv ab, bool& trap) {
+__device__ __forceinline__ double collision_body(Iv L, Iv S, Iv ab, bool& trap) {
     constexpr bool HI = (W == W_HI);
     if (L.lo < S.lo) L.lo = S.lo;
     if (L.hi < S.hi) S.hi = L.hi;
@@ -209,7 +221,16 @@ __device__ __noinline__ double collision(Iv L, Iv S, Iv ab, bool& trap) {
     double ob_val = HI ? -1.0 : 0.0;  // wanted bound of the partial result
     // for LO: what is needed to decide emptiness of the partial result lazily
     Iv lq{0, 0}, sq{0, 0};
+    bool lq_hi_lazy = false;
+    double ob_lx_hi = 0.0, ob_sx_lo = 0.0;
 
+    // Quotients whose only use is an emptiness or a domain test are not
+    // computed when an exact comparison decides that test (positive, proper
+    // operands in the certified division's range: `posq`).  For such x / o:
+    //   RD(x.lo / o.hi) > 1  <=>  x.lo >= o.hi * (1 + 2^-52)  (rd_quot_gt1)
+    //   RU(x.hi / o.lo) > 1  <=>  x.hi > o.lo
+    //   RD(x.lo / o.hi) >= 0 > -1,  and the quotient interval is proper.
+    // Every value and every trap decision is the one of the full evaluation.
     if (obt.pos) {
         Iv lx = iscale(0.5, iadd(add, ab));
         Iv sx = iscale(0.5, isub(add, ab));
@@ -218,6 +239,42 @@ __device__ __noinline__ double collision(Iv L, Iv S, Iv ab, bool& trap) {
         if (L.hi < lx.hi) lx.hi = L.hi;
         if (iempty(sx) || iempty(lx)) {
             if (obt.def) trap = true;
+        } else if (posq(lx, L) && posq(sx, S)) {
+            // lq = lx / L, sq = sx / S: proper, non-negative; after clamping the
+            // upper ends to 1, empty iff the lower end exceeds 1; no domain trap
+            if (W == W_TRAP) {
+                if (rd_quot_gt1(lx.lo, L.hi) || rd_quot_gt1(sx.lo, S.hi)) {
+                    if (obt.def) trap = true;
+                } else {
+                    ob_set = true;
+                }
+            } else if (HI) {
+                double lqh = div_ru(lx.hi, L.lo);
+                if (1.0 < lqh) lqh = 1.0;
+                const double sql = div_rd(sx.lo, S.hi);
+                if (rd_quot_gt1(lx.lo, L.hi) || sql > 1.0) {
+                    if (obt.def) trap = true;
+                } else {
+                    ob_set = true;
+                    ob_val = __dadd_ru(asin_ru(lqh), -asin_rd(sql));
+                }
+            } else {
+                const double lql = div_rd(lx.lo, L.hi);
+                double sqh = div_ru(sx.hi, S.lo);
+                if (1.0 < sqh) sqh = 1.0;
+                if (lql > 1.0 || rd_quot_gt1(sx.lo, S.hi)) {
+                    if (obt.def) trap = true;
+                } else {
+                    ob_set = true;
+                    lq.lo = lql;
+                    sq.hi = sqh;
+                    lq_hi_lazy = true;  // lq.hi and sq.lo: computed only if the join needs them
+                    ob_lx_hi = lx.hi;
+                    ob_sx_lo = sx.lo;
+                    ob_val = __dadd_rd(asin_rd(lql), -asin_ru(sqh));
+                    if (ob_val < 0.0) ob_val = 0.0;
+                }
+            }
         } else {
             lq = idiv(lx, L);
             if (1.0 < lq.hi) lq.hi = 1.0;
@@ -246,9 +303,14 @@ __device__ __noinline__ double collision(Iv L, Iv S, Iv ab, bool& trap) {
         if (iempty(sx)) {
             if (!obt.pos) trap = true;
         } else {
+            const bool fast = posq(lx, L) && posq(sx, S);
             if (W == W_TRAP) {
-                Iv alq = idiv(lx, L), asq = idiv(sx, S);
-                if (alq.lo < -1.0 || alq.hi > 1.0 || asq.lo < -1.0 || asq.hi > 1.0) trap = true;
+                if (fast) {
+                    if (lx.hi > L.lo || sx.hi > S.lo) trap = true;
+                } else {
+                    Iv alq = idiv(lx, L), asq = idiv(sx, S);
+                    if (alq.lo < -1.0 || alq.hi > 1.0 || asq.lo < -1.0 || asq.hi > 1.0) trap = true;
+                }
                 return 0.0;
             }
             double r;
@@ -259,11 +321,20 @@ __device__ __noinline__ double collision(Iv L, Iv S, Iv ab, bool& trap) {
                 if (!(sx.lo >= 0.0 && S.lo > 0.0) && idiv_lo(sx, S) < -1.0) trap = true;
                 r = __dadd_ru(asin_ru(lqh), asin_ru(sqh));
             } else {
-                Iv alq = idiv(lx, L), asq = idiv(sx, S);
-                if (alq.lo < -1.0 || alq.hi > 1.0 || asq.lo < -1.0 || asq.hi > 1.0) trap = true;
-                double b = asin_rd(asq.lo);
+                double alql, asql;
+                if (fast) {
+                    alql = div_rd(lx.lo, L.hi);
+                    asql = div_rd(sx.lo, S.hi);
+                    if (lx.hi > L.lo || sx.hi > S.lo) trap = true;
+                } else {
+                    Iv alq = idiv(lx, L), asq = idiv(sx, S);
+                    if (alq.lo < -1.0 || alq.hi > 1.0 || asq.lo < -1.0 || asq.hi > 1.0) trap = true;
+                    alql = alq.lo;
+                    asql = asq.lo;
+                }
+                double b = asin_rd(asql);
                 if (b < 0.0) b = 0.0;
-                r = __dadd_rd(asin_rd(alq.lo), b);
+                r = __dadd_rd(asin_rd(alql), b);
             }
             // result.empty() ? result = r : result.do_join(r)   (collision_angles.cu:108-112)
             bool ob_nonempty;
@@ -272,6 +343,11 @@ __device__ __noinline__ double collision(Iv L, Iv S, Iv ab, bool& trap) {
             } else if (HI) {
                 ob_nonempty = !(ob_val < 0.0);
             } else {
+                if (lq_hi_lazy) {
+                    lq.hi = div_ru(ob_lx_hi, L.lo);
+                    if (1.0 < lq.hi) lq.hi = 1.0;
+                    sq.lo = div_rd(ob_sx_lo, S.hi);
+                }
                 // empty  <=>  ru(asin_ru(lq.hi) - asin_rd(sq.lo)) < 0, which cannot hold when lq.hi >= sq.lo
                 ob_nonempty = (lq.hi >= sq.lo) || !(__dadd_ru(asin_ru(lq.hi), -asin_rd(sq.lo)) < 0.0);
             }
@@ -282,6 +358,26 @@ __device__ __noinline__ double collision(Iv L, Iv S, Iv ab, bool& trap) {
         }
     }
     return ob_val;
+}
+
+// One shared (not inlined) copy per Want.  The trap flag is a register of the
+// out-of-line function and comes back with the value: a flag passed by
+// reference into an out-of-line function would live in local memory.
+struct DTrap {
+    double v;
+    bool trap;
+};
+template <int W>
+__device__ __noinline__ DTrap collision_call(Iv L, Iv S, Iv ab) {
+    bool trap = false;
+    const double v = collision_body<W>(L, S, ab, trap);
+    return {v, trap};
+}
+template <int W>
+__device__ __forceinline__ double collision(Iv L, Iv S, Iv ab, bool& trap) {
+    const DTrap r = collision_call<W>(L, S, ab);
+    trap = trap || r.trap;
+    return r.v;
 }
 
 // collision_angles.cu:119-142.  TRAP_ONLY: evaluate only the trap sites.

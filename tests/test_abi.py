@@ -72,3 +72,24 @@ def test_reference_prover_links_against_shim(libpath, tmp_path):
     subprocess.run(["g++", "-std=c++17", f"-I{ref}/algcuda/cuda-cpp-wrapper/include", f"{ref}/prover.cpp",
                     f"-L{libdir}", "-lcp_b200", f"-Wl,-rpath,{libdir}", "-o", str(out)], check=True)
     assert out.exists()
+
+
+def test_proof_defaults_without_device(libpath):
+    """cp_proof_defaults needs no device: the seeds each family's proof uses."""
+    import ctypes
+
+    import circlepacking_b200 as cp
+
+    L = cp.lib()
+    L.cp_proof_defaults.argtypes = [ctypes.c_int, ctypes.POINTER(cp.ProofOpts)]
+    o = cp.ProofOpts()
+    assert L.cp_proof_defaults(9, ctypes.byref(o)) == 1  # CP_ERR_INVALID
+    assert L.cp_proof_defaults(0, ctypes.byref(o)) == 0
+    d = o.as_dict()
+    assert d["slabs"] == 18 and d["geometric"] == 1 and d["seed_sizes"] == [1, 256, 256, 64]
+    assert d["policy"] == 1 and d["engine"] == 1  # lambda-only split, graph engine
+    for f in range(1, 6):
+        assert L.cp_proof_defaults(f, ctypes.byref(o)) == 0
+        assert o.slabs == 1 and o.seed_sizes[0] == 64 and o.max_depth == 24
+    L.cp_prove_family.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    assert L.cp_prove_family(None, None, None) == 1
