@@ -225,9 +225,8 @@ __device__ __forceinline__ void tight_lo(EI& a, E x, bool&) { a.lo = emax(a.lo, 
 __device__ __forceinline__ void tight_hi(EI& a, E x, bool&) { a.hi = emin(a.hi, x); }
 
 // shadow of collision<W> (cp_fp64.cuh); trap events clear ok
-template <int W>
-__device__ __forceinline__ E collision_body(EI L, EI S, EI ab, bool& ok) {
-    constexpr bool HI = (W == W_HI);
+__device__ __forceinline__ E collision_body(EI L, EI S, EI ab, const int W, bool& ok) {
+    const bool HI = (W == W_HI);
     L.lo = emax(L.lo, S.lo);
     S.hi = emin(S.hi, L.hi);
     const EI l2 = isq(L, ok), s2 = isq(S, ok), a2 = isq(ab, ok);
@@ -342,15 +341,15 @@ struct EOk {
     E v;
     bool ok;
 };
-template <int W>
-__device__ __noinline__ EOk collision_call(EI L, EI S, EI ab) {
+// one copy for all three Wants (a runtime argument), for the instruction caches
+static __device__ __noinline__ EOk collision_call(EI L, EI S, EI ab, int W) {
     bool ok = true;
-    const E v = collision_body<W>(L, S, ab, ok);
+    const E v = collision_body(L, S, ab, W, ok);
     return {v, ok};
 }
 template <int W>
 __device__ __forceinline__ E collision(EI L, EI S, EI ab, bool& ok) {
-    const EOk r = collision_call<W>(L, S, ab);
+    const EOk r = collision_call(L, S, ab, W);
     ok = ok && r.ok;
     return r.v;
 }

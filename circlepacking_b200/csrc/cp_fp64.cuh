@@ -205,9 +205,8 @@ __device__ __forceinline__ bool rd_quot_gt1(double a, double b) {
 enum Want : int { W_LO = 0, W_HI = 1, W_TRAP = 2 };
 
 // compute_collision_angle (collision_angles.cu:37-117) for one Want.
-template <int W>
-__device__ __forceinline__ double collision_body(Iv L, Iv S, Iv ab, bool& trap) {
-    constexpr bool HI = (W == W_HI);
+__device__ __forceinline__ double collision_body(Iv L, Iv S, Iv ab, const int W, bool& trap) {
+    const bool HI = (W == W_HI);
     if (L.lo < S.lo) L.lo = S.lo;
     if (L.hi < S.hi) S.hi = L.hi;
     const Iv l2 = isq(L), s2 = isq(S), a2 = isq(ab);
@@ -360,22 +359,24 @@ __device__ __forceinline__ double collision_body(Iv L, Iv S, Iv ab, bool& trap) 
     return ob_val;
 }
 
-// One shared (not inlined) copy per Want.  The trap flag is a register of the
-// out-of-line function and comes back with the value: a flag passed by
-// reference into an out-of-line function would live in local memory.
+// The trap flag is a register of the out-of-line function and comes back with
+// the value: a flag passed by reference into an out-of-line function would
+// live in local memory.
 struct DTrap {
     double v;
     bool trap;
 };
-template <int W>
-__device__ __noinline__ DTrap collision_call(Iv L, Iv S, Iv ab) {
+// One copy for all three Wants (a runtime argument): the three template
+// copies of this long routine were the largest part of the level kernels'
+// instruction footprint.
+static __device__ __noinline__ DTrap collision_call(Iv L, Iv S, Iv ab, int W) {
     bool trap = false;
-    const double v = collision_body<W>(L, S, ab, trap);
+    const double v = collision_body(L, S, ab, W, trap);
     return {v, trap};
 }
 template <int W>
 __device__ __forceinline__ double collision(Iv L, Iv S, Iv ab, bool& trap) {
-    const DTrap r = collision_call<W>(L, S, ab);
+    const DTrap r = collision_call(L, S, ab, W);
     trap = trap || r.trap;
     return r.v;
 }
