@@ -562,8 +562,15 @@ cp_status refine_levels(cp_prover* p, const cp_refine_opts& o, cp_refine_report*
         if (cp_model_collecting(p))
             CP_TRY(cp_model_collect_chunk(p, fam, in.b, begin, c, p->tab_t, p->tab_v, p->tab_n, p->tab_h));
         if (o.policy == CP_SPLIT_LEARNED || o.learned_order) {
+            // the inference launch is part of the refinement's device time
+            CP_TRY(cuda_ok(cudaEventRecord(p->ev0, p->stream)));
             CP_TRY(cp_model_hints(p, fam, in.b, begin, c, o.policy == CP_SPLIT_LEARNED ? &axis : nullptr,
                                   o.learned_order ? &order : nullptr));
+            CP_TRY(cuda_ok(cudaEventRecord(p->ev1, p->stream)));
+            CP_TRY(cuda_ok(cudaEventSynchronize(p->ev1)));
+            float t = 0;
+            cudaEventElapsedTime(&t, p->ev0, p->ev1);
+            ms += t;
         }
         CP_TRY(cp_engine_eval_chunk(p, fam, o, in, begin, c, out, axis, order, &ms));
         ++launches;
@@ -658,9 +665,28 @@ cp_status build_graph(cp_prover* p, const cp_refine_opts& o, int variant, int bp
         const int block = net ? kNetBlock : kGraphBlock[variant];
         int per_sm = 0, sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
-        // each CTA of the inline-network kernel holds tc::kNetCols tensor-memory columns
-        if (net && per_sm > kNetMaxCtasPerSm) per_sm = kNetMaxCtasPerSm;
+        if (net) {
+            // The occupancy calculator reports one CTA per SM for the kernel that
+            // uses tensor memory, while the SM keeps as many resident as its
+            // registers, shared memory (about 32 KB per CTA, largest carveout)
+            // and tensor memory (tc::kNetCols columns per CTA) allow; the grid is
+            // sized from those limits.  A CTA beyond the resident ones starts when
+            // one ends (the kernel claims work dynamically), so an overestimate
+            // costs a few idle CTAs, never a wait on one another.
+            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+            cudaFuncAttributes fa{};
+            int regs_sm = 65536, smem_sm = 0;
+            cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, p->device);
+            cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, p->device);
+            if (cudaFuncGetAttributes(&fa, kern) == cudaSuccess && fa.numRegs > 0) {
+                const int by_regs = regs_sm / (((fa.numRegs + 7) / 8 * 8) * block);
+                const int by_smem = smem_sm / ((int)fa.sharedSizeBytes + 1024);  // 1 KB reserved per CTA
+                per_sm = std::min(std::min(by_regs, by_smem), kNetMaxCtasPerSm);
+            }
+            if (per_sm < 1) per_sm = 1;
+        } else if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0) != cudaSuccess || per_sm < 1) {
+            per_sm = 1;
+        }
         void* args[] = {&pa};
         void* net_args[] = {&pa, &na};
         st = cuda_ok(cudaLaunchKernel(kern, dim3((unsigned)(sms * per_sm)), dim3((unsigned)block), net ? net_args : args,

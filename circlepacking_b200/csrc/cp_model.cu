@@ -664,8 +664,7 @@ __global__ void __launch_bounds__(kTcRows) k_infer_tc(TcArgs ta) {
 #pragma unroll
                 for (int k = 0; k < 16; ++k) f[k] = 0.f;
             }
-#pragma unroll
-            for (int k = 0; k < 16; ++k) s.a[cm_off(tid, k, NK)] = __float2bfloat16_rn(f[k]);
+            put_row_bf16<NK>(s.a, tid, 0, NK, f);
         }
         uint32_t r[64];
 #pragma unroll
@@ -688,7 +687,7 @@ __global__ void __launch_bounds__(kTcRows) k_infer_tc(TcArgs ta) {
                 }
                 tc_commit(mbar);
             }
-            ok = __syncthreads_and(mbar_wait(mbar, phase, ta.wait_limit) ? 1 : 0) != 0;  // block-uniform
+            ok = __syncthreads_and(tc_wait_one(mbar, phase, ta.wait_limit)) != 0;  // block-uniform
             // the parity advances only past a completed phase: after a time-out
             // `phase` still names the pending one, which the drain below waits for
             if (ok) phase ^= 1u;
@@ -699,9 +698,8 @@ __global__ void __launch_bounds__(kTcRows) k_infer_tc(TcArgs ta) {
                 const float* bias = layer == 0 ? s.b1 : s.b2;
                 tc_fence_before();
                 __syncthreads();  // every thread has read its row; the tile may be overwritten
-#pragma unroll
-                for (int c = 0; c < NH; ++c)
-                    s.a[cm_off(tid, c, NH)] = __float2bfloat16_rn(gelu_fast(__uint_as_float(r[c]) + bias[c]));
+                gelu_row32(s.a, tid, 0, r, bias);
+                gelu_row32(s.a, tid, 32, r + 32, bias);
             } else {
                 tc_ld16(tmem + lane_base + 64u, r);
             }
@@ -879,7 +877,7 @@ __global__ void __launch_bounds__(kTcRows) k_train_tc(TtArgs ta) {
             }
             tc_commit(mbar);
         }
-        const bool done = __syncthreads_and(mbar_wait(mbar, phase, ta.wait_limit) ? 1 : 0) != 0;  // block-uniform
+        const bool done = __syncthreads_and(tc_wait_one(mbar, phase, ta.wait_limit)) != 0;  // block-uniform
         if (done) phase ^= 1u;  // after a time-out `phase` names the pending phase (drained below)
         tc_fence_after();
         return done;
@@ -1287,6 +1285,9 @@ template <int FAM>
 cp_status launch_infer_tc_t(const TcArgs& a, cudaStream_t st) {
     const size_t tiles = (a.a.count + kTcRows - 1) / kTcRows;
     const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(tiles, 148 * 4));
+    // about 30 KB of static shared memory per CTA: the largest carveout lets the
+    // four CTAs per SM that the tensor memory allows (128 columns each) be resident
+    cudaFuncSetAttribute(k_infer_tc<FAM>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     k_infer_tc<FAM><<<grid, kTcRows, 0, st>>>(a);
     return cp_check_launch();
 }

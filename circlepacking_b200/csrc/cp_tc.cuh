@@ -62,6 +62,40 @@ __device__ __forceinline__ int cm_off(int row, int k, int K) {
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
+// Writes N values (N a multiple of 8) of one row of a K-major core-matrix tile,
+// from column k0 (a multiple of 8): each group of 8 columns of a row is 16
+// contiguous bytes, written as one 16-byte store of 8 BF16 values (round to
+// nearest even, as __float2bfloat16_rn).
+template <int N>
+__device__ __forceinline__ void put_row_bf16(bf16* tile, int row, int k0, int K, const float* v) {
+#pragma unroll
+    for (int g = 0; g < N / 8; ++g) {
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const __nv_bfloat162 h = __floats2bfloat162_rn(v[8 * g + 2 * q], v[8 * g + 2 * q + 1]);  // .x: lower column
+            w[q] = *reinterpret_cast<const uint32_t*>(&h);
+        }
+        *reinterpret_cast<uint4*>(tile + cm_off(row, k0 + 8 * g, K)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+// Hidden-layer epilogue of 32 accumulators of one row: bias + GELU, written as
+// BF16 to columns k0..k0+31 of the next operand tile (K = NH).  The biases are
+// read into registers before any store, so the 32 independent chains overlap.
+__device__ __forceinline__ void gelu_row32(bf16* tile, int row, int k0, const uint32_t* r, const float* bias) {
+    float v[32];
+#pragma unroll
+    for (int c = 0; c < 32; c += 4) {
+        const float4 b = *reinterpret_cast<const float4*>(bias + k0 + c);
+        v[c] = __uint_as_float(r[c]) + b.x;
+        v[c + 1] = __uint_as_float(r[c + 1]) + b.y;
+        v[c + 2] = __uint_as_float(r[c + 2]) + b.z;
+        v[c + 3] = __uint_as_float(r[c + 3]) + b.w;
+    }
+#pragma unroll
+    for (int c = 0; c < 32; ++c) v[c] = gelu_fast(v[c]);
+    put_row_bf16<32>(tile, row, k0, NH, v);
+}
 // shared-memory matrix descriptor (no swizzle, K-major), Blackwell version 1
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
     return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
@@ -95,6 +129,15 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, int lim
         if (done) return true;
     }
     return false;
+}
+// Block-collective completion wait: thread 0 alone polls the mbarrier (so the
+// block's other warps take no issue slots from co-resident warps while the
+// product runs) and returns 1 when the phase completed within `limit` polls;
+// the caller makes the result block-uniform with __syncthreads_and, whose
+// barrier orders the other threads after thread 0's observation, and issues
+// tcgen05.fence::after_thread_sync before reading the accumulators.
+__device__ __forceinline__ int tc_wait_one(uint32_t mbar, uint32_t phase, int limit) {
+    return threadIdx.x == 0 ? (mbar_wait(mbar, phase, limit) ? 1 : 0) : 1;
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -171,8 +214,7 @@ __device__ __forceinline__ void net_setup(NetSmem& s, const bf16* __restrict__ v
 __device__ __forceinline__ bool net_forward(NetSmem& s, const float* f, float* z, int wait_limit) {
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-#pragma unroll
-    for (int k = 0; k < NK; ++k) s.a[cm_off(tid, k, NK)] = __float2bfloat16_rn(f[k]);
+    put_row_bf16<NK>(s.a, tid, 0, NK, f);
     const uint32_t mbar = smem_u32(&s.mbar);
     uint32_t r[32];
     for (int layer = 0; layer < 3; ++layer) {
@@ -195,7 +237,7 @@ __device__ __forceinline__ bool net_forward(NetSmem& s, const float* f, float* z
             }
             tc_commit(mbar);
         }
-        const bool ok = __syncthreads_and(mbar_wait(mbar, phase, wait_limit) ? 1 : 0) != 0;  // block-uniform
+        const bool ok = __syncthreads_and(tc_wait_one(mbar, phase, wait_limit)) != 0;  // block-uniform
         tc_fence_after();
         if (!ok) return false;  // s.phase still names the pending phase
         __syncthreads();        // every thread has read s.phase
@@ -207,10 +249,7 @@ __device__ __forceinline__ bool net_forward(NetSmem& s, const float* f, float* z
 #pragma unroll
             for (int half = 0; half < 2; ++half) {
                 tc_ld32(tmem + lane_base + 32u * half, r);
-#pragma unroll
-                for (int c = 0; c < 32; ++c)
-                    s.a[cm_off(tid, 32 * half + c, NH)] =
-                        __float2bfloat16_rn(gelu_fast(__uint_as_float(r[c]) + bias[32 * half + c]));
+                gelu_row32(s.a, tid, 32 * half, r, bias);
             }
         } else {
             tc_ld16(tmem + lane_base, r);
