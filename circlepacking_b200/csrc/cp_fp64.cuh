@@ -428,10 +428,12 @@ __device__ __forceinline__ double ca_mixed_corner(Iv la, double a, double b, boo
     Iv ab{__dadd_rd(a, b), __dadd_ru(a, b)};
     const bool def_ca_longer = cb.hi <= ca.lo;
     const bool pos_ca_longer = cb.lo <= ca.hi;
-    if (def_ca_longer) return collision<W>(ca, cb, ab, trap);
-    if (!pos_ca_longer) return collision<W>(cb, ca, ab, trap);
-    double r1 = collision<W>(ca, cb, ab, trap);
-    double r2 = collision<W>(cb, ca, ab, trap);
+    // one call site for the first (or only) ordering, so the lanes of a warp
+    // that take different orderings evaluate it together
+    const bool swap = !def_ca_longer && !pos_ca_longer;  // cb is definitely the longer side
+    const double r1 = collision<W>(swap ? cb : ca, swap ? ca : cb, ab, trap);
+    if (def_ca_longer || swap) return r1;
+    const double r2 = collision<W>(cb, ca, ab, trap);
     return (W == W_HI) ? (r2 > r1 ? r2 : r1) : (r2 < r1 ? r2 : r1);
 }
 // collision_angles.cu:160-173 (OUTER_FIRST) and 191-205: lower bound is 0 when

@@ -105,10 +105,13 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
     unsigned nchild = 0;
     double lo[4], hi[4];
     int depth = 0, axis = 0;
+    int v = -1;                 // this lane's verdict (-1: no box evaluated)
+    bool clipped = false, unresolved = false, fp32_decided = false;
+    unsigned long long h = 0;   // digest hash of (box, verdict)
     if (j < a.count) {
         depth = a.in.depth[i];
         if (depth == 0xFF) {
-            atomicAdd(&sm.hist[C_CLIPPED], 1ull);
+            clipped = true;
         } else {
 #pragma unroll
             for (int d = 0; d < D; ++d) {
@@ -116,7 +119,6 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                 hi[d] = a.in.hi[d * a.in.cap + i];
             }
             const int ord = ord_in >= 0 ? ord_in : (a.order_hint ? a.order_hint[j] : 0);
-            int v;
             if (PREC == CP_FP32_PREFILTER) {
                 uint8_t pmask;
                 const int pre = prefilter_box<FAM>(lo, hi, ord, false, &pmask);
@@ -126,23 +128,17 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                     handles += r.handles;
                 } else {
                     v = pre == PF_PROVED ? V_PROVED : pre == PF_EMPTY ? V_EMPTY : pre == PF_NOFIT ? V_NOFIT : V_CRITICAL;
-                    if (pre != PF_EMPTY) atomicAdd(&sm.hist[C_FP32], 1ull);
+                    fp32_decided = pre != PF_EMPTY;
                 }
             } else {
                 const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr);
                 v = r.verdict;
                 handles += r.handles;
             }
-            atomicAdd(&sm.hist[v], 1ull);
-            atomicAdd(&sm.depth[depth < kDepthBins ? depth : kDepthBins - 1], 1ull);
-            if (a.digest) {
-                const unsigned long long h = box_hash<D>(lo, hi, v);
-                atomicAdd(&sm.dig_sum, h);
-                atomicXor(&sm.dig_xor, mix64(h ^ 0x5851f42d4c957f2dull));
-            }
+            if (a.digest) h = box_hash<D>(lo, hi, v);
             if (v != V_PROVED && v != V_EMPTY) {
                 if (depth >= a.max_depth) {
-                    atomicAdd(&sm.hist[C_UNRESOLVED], 1ull);
+                    unresolved = true;
                 } else {
                     nchild = fanout(a.policy, D);
                     if (a.policy == SPLIT_WIDEST)
@@ -152,6 +148,40 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                     else if (a.policy == SPLIT_GIVEN)
                         axis = axis_in >= 0 ? axis_in % D : (a.axis_hint ? (a.axis_hint[j] % D) : 0);
                 }
+            }
+        }
+    }
+    // counts, once per warp (all 32 lanes are here): one shared-memory atomic
+    // per verdict, depth and flag present in the warp instead of one per box
+    {
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const unsigned b = __ballot_sync(0xffffffffu, v == k);
+            if (b && lane == 0) atomicAdd(&sm.hist[k], (unsigned long long)__popc(b));
+        }
+        const unsigned bc = __ballot_sync(0xffffffffu, clipped);
+        const unsigned bu = __ballot_sync(0xffffffffu, unresolved);
+        const unsigned bf = __ballot_sync(0xffffffffu, fp32_decided);
+        if (lane == 0) {
+            if (bc) atomicAdd(&sm.hist[C_CLIPPED], (unsigned long long)__popc(bc));
+            if (bu) atomicAdd(&sm.hist[C_UNRESOLVED], (unsigned long long)__popc(bu));
+            if (bf) atomicAdd(&sm.hist[C_FP32], (unsigned long long)__popc(bf));
+        }
+        const int dbin = v >= 0 ? (depth < kDepthBins ? depth : kDepthBins - 1) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, dbin);
+        if (dbin >= 0 && lane == __ffs(peers) - 1) atomicAdd(&sm.depth[dbin], (unsigned long long)__popc(peers));
+        if (a.digest) {
+            unsigned long long hs = v >= 0 ? h : 0ull;
+            unsigned long long hx = v >= 0 ? mix64(h ^ 0x5851f42d4c957f2dull) : 0ull;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                hs += __shfl_xor_sync(0xffffffffu, hs, off);
+                hx ^= __shfl_xor_sync(0xffffffffu, hx, off);
+            }
+            if (lane == 0) {
+                atomicAdd(&sm.dig_sum, hs);
+                atomicXor(&sm.dig_xor, hx);
             }
         }
     }
