@@ -194,7 +194,8 @@ class RefineOpts(ctypes.Structure):
                 ("max_depth", ctypes.c_int32), ("seed_sizes", ctypes.c_int32 * 4), ("seed_lambda", ctypes.c_double * 2),
                 ("level_capacity", ctypes.c_int64), ("block", ctypes.c_int32), ("learned_order", ctypes.c_int32),
                 ("engine", ctypes.c_int32), ("boxes_per_thread", ctypes.c_int32), ("lambda_scale", ctypes.c_double),
-                ("digest", ctypes.c_int32), ("seed_parts", ctypes.c_int32), ("seed_part", ctypes.c_int32)]
+                ("digest", ctypes.c_int32), ("seed_parts", ctypes.c_int32), ("seed_part", ctypes.c_int32),
+                ("reuse", ctypes.c_int32)]
 
 
 class RefineReport(ctypes.Structure):
@@ -226,7 +227,8 @@ class ProofOpts(ctypes.Structure):
     _fields_ = [("family", ctypes.c_int32), ("precision", ctypes.c_int32), ("engine", ctypes.c_int32),
                 ("policy", ctypes.c_int32), ("max_depth", ctypes.c_int32), ("slabs", ctypes.c_int32),
                 ("geometric", ctypes.c_int32), ("seed_sizes", ctypes.c_int32 * 4), ("level_capacity", ctypes.c_int64),
-                ("digest", ctypes.c_int32), ("seed_parts", ctypes.c_int32), ("seed_part", ctypes.c_int32)]
+                ("digest", ctypes.c_int32), ("seed_parts", ctypes.c_int32), ("seed_part", ctypes.c_int32),
+                ("reuse", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: (list(getattr(self, k)) if k == "seed_sizes" else getattr(self, k)) for k, _ in self._fields_}
@@ -364,7 +366,7 @@ class Prover:
     @staticmethod
     def opts(family, precision=FP64, policy=SPLIT_UNIFORM, max_depth=2, seed_sizes=None, seed_lambda=None,
              level_capacity=0, learned_order=False, engine=ENGINE_LEVELS, block=0, boxes_per_thread=0,
-             lambda_scale=0.0, digest=False, seed_part=0, seed_parts=1) -> RefineOpts:
+             lambda_scale=0.0, digest=False, seed_part=0, seed_parts=1, reuse=True) -> RefineOpts:
         o = RefineOpts()
         o.family, o.precision, o.policy, o.max_depth = family, precision, policy, max_depth
         ss = list(seed_sizes or [64] * DIMS[family]) + [1] * 4
@@ -380,6 +382,7 @@ class Prover:
         o.lambda_scale = lambda_scale
         o.digest = int(bool(digest))
         o.seed_parts, o.seed_part = seed_parts, seed_part
+        o.reuse = int(bool(reuse))
         return o
 
     def autotune(self, family, **kw):

@@ -283,8 +283,9 @@ double now_ms() {
 
 // ------------------------------------------------------------------ handle
 struct LevelBuf {
-    BoxList b{nullptr, nullptr, nullptr, 0};
+    BoxList b{nullptr, nullptr, nullptr, 0, nullptr};
     size_t n = 0;
+    double* aux = nullptr;  // kAuxFields x cap, allocated on first use (b.aux points here when in use)
 };
 
 struct cp_prover {
@@ -358,6 +359,7 @@ void free_levels(cp_prover* p) {
         cudaFree(L.b.lo);
         cudaFree(L.b.hi);
         cudaFree(L.b.depth);
+        cudaFree(L.aux);
     }
     p->levels.clear();
 }
@@ -391,8 +393,8 @@ cp_status ensure_slab(cp_prover* p, int n) {
 SingleTable table_of(const cp_prover* p) { return SingleTable{p->tab_t, p->tab_v, p->tab_n, p->tab_h}; }
 
 using LevelKernel = void (*)(LevelArgs);
+// register variants of the level kernel: minimum resident blocks 1, 4, 5, 6
 constexpr int kVariants = 4;
-constexpr int kVariantMinBlocks[kVariants] = {1, 4, 5, 6};
 template <int FAM, int PREC>
 LevelKernel level_variant(int v) {
     switch (v) {
@@ -762,7 +764,26 @@ cp_status refine_graph(cp_prover* p, const cp_refine_opts& o, cp_refine_report* 
     return CP_OK;
 }
 
+// The lambda-independent terms of the start family travel with the boxes of
+// levels >= 1 (children) when the refinement asks for it (opts.reuse) and its
+// split can leave radii unchanged; every other refinement, and the seed level,
+// sees no aux.  A level whose aux cannot
+// be allocated goes without: its boxes recompute the terms.
+void attach_aux(cp_prover* p, const cp_refine_opts& o) {
+    // a uniform split changes every radius of every child: nothing to carry
+    const bool use = o.reuse != 0 && o.family == F_START && o.policy != CP_SPLIT_UNIFORM;
+    for (size_t l = 0; l < p->levels.size(); ++l) {
+        LevelBuf& L = p->levels[l];
+        if (use && l > 0 && !L.aux && cudaMalloc(&L.aux, sizeof(double) * kAuxFields * L.b.cap) != cudaSuccess) {
+            L.aux = nullptr;
+            cudaGetLastError();  // clear the allocation error
+        }
+        L.b.aux = (use && l > 0) ? L.aux : nullptr;
+    }
+}
+
 cp_status run_refinement(cp_prover* p, const cp_refine_opts& o, cp_refine_report* r, double t0) {
+    attach_aux(p, o);
     if (o.engine == CP_ENGINE_GRAPH && !cp_model_collecting(p)) return refine_graph(p, o, r, t0);
     return refine_levels(p, o, r, t0);
 }
@@ -929,6 +950,7 @@ cp_status cp_proof_defaults(int family, cp_proof_opts* o) {
     o->slabs = 1;
     o->geometric = 0;
     o->level_capacity = (int64_t)1 << 23;
+    o->reuse = 1;
     // the radius resolution each family's lambda-only proof needs, with 64
     // lambda cells over the whole range; start: geometric lambda slabs with the
     // reference's own radius lattice per slab (start_configuration.cu:41-44)
@@ -969,6 +991,7 @@ cp_status cp_prove_family(cp_prover* p, const cp_proof_opts* o, cp_proof_report*
         ro.digest = o->digest;
         ro.seed_parts = o->seed_parts;
         ro.seed_part = o->seed_part;
+        ro.reuse = o->reuse;
         cp_refine_report rr;
         const cp_status s = cp_refine_keep_interrupt(p, &ro, &rr);
         if (s != CP_OK) {
@@ -1254,6 +1277,9 @@ cp_status cp_checkpoint_load(cp_prover* p, const char* path, cp_refine_opts* opt
         for (uint32_t d = 0; d < h.dims; ++d) CP_TRY(load(fc.f, b.lo + d * b.cap, n[l], stage, p->stream));
         for (uint32_t d = 0; d < h.dims; ++d) CP_TRY(load(fc.f, b.hi + d * b.cap, n[l], stage, p->stream));
         CP_TRY(load(fc.f, b.depth, n[l], stage, p->stream));
+        // a checkpoint carries no lambda-independent terms: the loaded boxes recompute them
+        if (p->levels[l].aux)
+            CP_TRY(cuda_ok(cudaMemsetAsync(p->levels[l].aux + 3 * b.cap, 0, sizeof(double) * n[l], p->stream)));
         p->levels[l].n = (size_t)n[l];
     }
     p->pending = true;

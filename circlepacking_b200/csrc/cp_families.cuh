@@ -28,6 +28,17 @@ struct Verdict {
     uint8_t handles;  // guarded criteria (handles) evaluated for this box
 };
 
+// The terms of the start family's criteria that do not depend on lambda
+// (start_configuration.cu:126-162): the collision angle of disks 1 and 3 on the
+// outer border, ca_outer_outer(r1, r3), and the upper semicircle angle of r1.
+// They are functions of the radii alone (r1 tightened by r2 and r3), so a box
+// whose radii equal its parent's bit for bit has its parent's values.
+// flag: 0 = not available, 1 = available, 2 = available and their evaluation
+// reached a trap site.
+struct LaFree {
+    double a13lo, a13hi, so_hi, flag;
+};
+
 enum EvalMode { FULL = 0, DECIDE = 1 };
 
 __device__ __forceinline__ void trace_put(double* tr, int k, double lhs, double rhs) {
@@ -222,8 +233,11 @@ __device__ __noinline__ HandleOut end3d_handle_call(Iv la, Iv r1, Iv r2, Iv r3) 
 // order: for the families with two independent handles (middle, end_2d,
 // end_3d) bit 0 set = evaluate the second handle first (DECIDE mode only).
 // tr: FULL mode only, 16 doubles (lhs, rhs per sub-criterion) or nullptr.
+// la_in / la_out (start family, optional): the lambda-independent terms of this
+// box when already known (la_in->flag != 0), and where to report them.
 template <int FAM, int MODE>
-__device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, int order, double* tr) {
+__device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, int order, double* tr,
+                                            const LaFree* la_in = nullptr, LaFree* la_out = nullptr) {
     constexpr int D = family_dims(FAM);
     Iv la{lo[0], hi[0]}, r1{lo[1], hi[1]}, r2{lo[2], hi[2]}, r3{0.0, 0.0};
     if (D == 4) {
@@ -247,13 +261,25 @@ __device__ __forceinline__ Verdict eval_box(const double* lo, const double* hi, 
 
     if (FAM == F_START) {
         const Iv a12 = ca_outer_inner(la, r1, r2, trap);
-        const Iv a13 = ca_outer_outer(r1, r3, trap);
+        Iv a13;
+        double so_hi;
+        if (la_in && la_in->flag != 0.0) {
+            a13 = {la_in->a13lo, la_in->a13hi};
+            so_hi = la_in->so_hi;
+            if (la_in->flag == 2.0) trap = true;
+            if (la_out) *la_out = *la_in;
+        } else {
+            bool t13 = false;
+            a13 = ca_outer_outer(r1, r3, t13);
+            so_hi = semi_outer_hi(r1);
+            if (t13) trap = true;
+            if (la_out) *la_out = {a13.lo, a13.hi, so_hi, t13 ? 2.0 : 1.0};
+        }
         const Iv a23 = ca_inner_outer(la, r2, r3, trap);
         const Iv s = iadd(a12, a23);
         const Ub case1{a13.hi < s.lo, a13.lo < s.hi};  // a12 + a23 > a13
         const double ratio = area_ratio_ub(la);
         const double ar1 = disk_area_lb(r1), ar2 = disk_area_lb(r2);
-        const double so_hi = semi_outer_hi(r1);
         if (case1.pos) {
             ++handles;
             double used = used_ub(ratio, __dadd_ru(so_hi, a12.hi));

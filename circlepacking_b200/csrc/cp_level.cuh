@@ -106,6 +106,7 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
     double lo[4], hi[4];
     int depth = 0, axis = 0;
     int v = -1;                 // this lane's verdict (-1: no box evaluated)
+    LaFree lf{0.0, 0.0, 0.0, 0.0};  // start family: the box's lambda-independent terms, when known
     bool clipped = false, unresolved = false, fp32_decided = false;
     unsigned long long h = 0;   // digest hash of (box, verdict)
     if (j < a.count) {
@@ -119,11 +120,21 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                 hi[d] = a.in.hi[d * a.in.cap + i];
             }
             const int ord = ord_in >= 0 ? ord_in : (a.order_hint ? a.order_hint[j] : 0);
+            LaFree lin{0.0, 0.0, 0.0, 0.0};
+            if (FAM == F_START && a.in.aux) {
+                lin.flag = a.in.aux[3 * a.in.cap + i];
+                if (lin.flag != 0.0) {
+                    lin.a13lo = a.in.aux[i];
+                    lin.a13hi = a.in.aux[a.in.cap + i];
+                    lin.so_hi = a.in.aux[2 * a.in.cap + i];
+                }
+                lf = lin;
+            }
             if (PREC == CP_FP32_PREFILTER) {
                 uint8_t pmask;
                 const int pre = prefilter_box<FAM>(lo, hi, ord, false, &pmask);
                 if (pre == PF_UNDECIDED) {
-                    const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr);
+                    const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr, &lin, &lf);
                     v = r.verdict;
                     handles += r.handles;
                 } else {
@@ -131,7 +142,7 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                     fp32_decided = pre != PF_EMPTY;
                 }
             } else {
-                const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr);
+                const Verdict r = eval_box<FAM, DECIDE>(lo, hi, ord, nullptr, &lin, &lf);
                 v = r.verdict;
                 handles += r.handles;
             }
@@ -211,6 +222,13 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                 const int c = (int)k - (int)__shfl_sync(0xffffffffu, excl, own);
                 const int pax = __shfl_sync(0xffffffffu, axis, own);
                 const int pdep = __shfl_sync(0xffffffffu, depth, own);
+                LaFree plf{0.0, 0.0, 0.0, 0.0};
+                if (FAM == F_START && a.out.aux) {
+                    plf.a13lo = __shfl_sync(0xffffffffu, lf.a13lo, own);
+                    plf.a13hi = __shfl_sync(0xffffffffu, lf.a13hi, own);
+                    plf.so_hi = __shfl_sync(0xffffffffu, lf.so_hi, own);
+                    plf.flag = __shfl_sync(0xffffffffu, lf.flag, own);
+                }
                 if (valid) {
                     make_child<D>(plo, phi, a.policy, pax, c, clo, chi);
                     const bool alive = clip_child<FAM>(clo, chi, a.tab);
@@ -221,6 +239,20 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                         a.out.hi[d * a.out.cap + o] = chi[d];
                     }
                     a.out.depth[o] = alive ? (uint8_t)(pdep + 1) : (uint8_t)0xFF;
+                    if (FAM == F_START && a.out.aux) {
+                        // the parent's terms hold for the child when its radii are the parent's, bit for bit
+                        bool same = plf.flag != 0.0;
+#pragma unroll
+                        for (int d = 1; d < D; ++d)
+                            same = same && __double_as_longlong(clo[d]) == __double_as_longlong(plo[d]) &&
+                                   __double_as_longlong(chi[d]) == __double_as_longlong(phi[d]);
+                        a.out.aux[3 * a.out.cap + o] = same ? plf.flag : 0.0;
+                        if (same) {
+                            a.out.aux[o] = plf.a13lo;
+                            a.out.aux[a.out.cap + o] = plf.a13hi;
+                            a.out.aux[2 * a.out.cap + o] = plf.so_hi;
+                        }
+                    }
                 }
             }
             __syncwarp();

@@ -7,12 +7,17 @@
 namespace cpb {
 
 // Structure-of-arrays box list: axis d of box i is lo[d*cap + i] / hi[d*cap + i].
+// aux (optional, start family): the lambda-independent criterion terms of box
+// i, LaFree field k at aux[k*cap + i] (a13.lo, a13.hi, semi-angle of r1, flag),
+// carried from a box to those of its children whose radii are unchanged.
 struct BoxList {
     double* lo;
     double* hi;
     uint8_t* depth;
     size_t cap;
+    double* aux;
 };
+constexpr int kAuxFields = 4;
 
 // Split policies (how a not-proved box is refined)
 enum SplitPolicy : int {

@@ -203,6 +203,11 @@ typedef struct cp_refine_opts {
     int32_t seed_part;      /* ... and refines piece seed_part only: lattice boxes seed_part + k * seed_parts
                                (one rank's share of the same proof; the pieces' reports add up to the
                                whole seed's, digests included) */
+    int32_t reuse;          /* start family: 1 = a child whose radii equal its parent's (every child of a
+                               lambda-only split that clipping leaves alone) takes the parent's
+                               lambda-independent criterion terms instead of recomputing them (same
+                               values bit for bit; 32 B more per box in the levels above the seed);
+                               0 = every box computes every term */
 } cp_refine_opts;
 
 /* Refinement engines.  CP_ENGINE_LEVELS: the host picks each chunk, launches
@@ -271,6 +276,7 @@ typedef struct cp_proof_opts {
     int32_t digest;          /* 1 = per-box verdict digest in the report */
     int32_t seed_parts;      /* > 1: refine only the interleaved piece seed_part of every slab's lattice */
     int32_t seed_part;       /* (one rank's share of the proof, see cp_refine_opts) */
+    int32_t reuse;           /* see cp_refine_opts.reuse (cp_proof_defaults: 1) */
 } cp_proof_opts;
 
 typedef struct cp_proof_report {

@@ -7,13 +7,17 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-KEYS = ("evaluated", "verdicts", "unresolved", "clipped", "fp32_decided", "per_depth", "handles_evaluated")
+KEYS = ("evaluated", "verdicts", "unresolved", "clipped", "fp32_decided", "per_depth", "handles_evaluated", "digest")
 
 
-@pytest.mark.parametrize("family,policy", [(3, 2), (5, 1), (4, 0)])
+# (0, 1): the start family with a lambda-only split carries its parents'
+# lambda-independent terms in the levels; a checkpoint does not hold them, so
+# the resumed boxes recompute them
+@pytest.mark.parametrize("family,policy", [(3, 2), (5, 1), (4, 0), (0, 1)])
 def test_interrupt_resume_and_checkpoint(cp, tmp_path, family, policy):
     d = cp.DIMS[family]
-    kw = dict(policy=policy, max_depth=8 if policy else 3, seed_sizes=[16, 8, 8, 4][:d], level_capacity=1 << 16)
+    kw = dict(policy=policy, max_depth=8 if policy else 3, seed_sizes=[16, 8, 8, 4][:d], level_capacity=1 << 16,
+              digest=True)
     p = cp.Prover(0)
     try:
         want = p.refine(family, **kw)
