@@ -288,7 +288,8 @@ def proof_leg(prover, cp, forms, families, world=1):
         # the plain form recomputes every criterion term of every box (no reuse of
         # a parent's lambda-independent terms)
         plain_kw = dict(best_kw, engine=cp.ENGINE_LEVELS, precision=cp.FP64, reuse=0)
-        prover.prove_family(f, **dict(best_kw, slabs=1, seed_sizes=[4, 4, 4, 4]))  # warm-up (graph build)
+        # warm-up (graph build): one slab of a 4^dims seed as given, no per-slab scaling
+        prover.prove_family(f, **dict(best_kw, slabs=1, seed_sizes=[4, 4, 4, 4], slab_scale=[0] * 32))
         b = prover.prove_family(f, **best_kw)
         p = prover.prove_family(f, **plain_kw)
         same = (b["digest"] == p["digest"] and b["verdicts"] == p["verdicts"] and b["per_depth"] == p["per_depth"]

@@ -228,10 +228,11 @@ class ProofOpts(ctypes.Structure):
                 ("policy", ctypes.c_int32), ("max_depth", ctypes.c_int32), ("slabs", ctypes.c_int32),
                 ("geometric", ctypes.c_int32), ("seed_sizes", ctypes.c_int32 * 4), ("level_capacity", ctypes.c_int64),
                 ("digest", ctypes.c_int32), ("seed_parts", ctypes.c_int32), ("seed_part", ctypes.c_int32),
-                ("reuse", ctypes.c_int32)]
+                ("reuse", ctypes.c_int32), ("slab_scale", ctypes.c_int32 * 32)]
 
     def as_dict(self) -> dict:
-        return {k: (list(getattr(self, k)) if k == "seed_sizes" else getattr(self, k)) for k, _ in self._fields_}
+        return {k: (list(getattr(self, k)) if k in ("seed_sizes", "slab_scale") else getattr(self, k))
+                for k, _ in self._fields_}
 
 
 class ProofReport(ctypes.Structure):
@@ -461,6 +462,10 @@ class Prover:
                 ss = list(v) + [1] * 4
                 for d in range(4):
                     o.seed_sizes[d] = ss[d]
+            elif k == "slab_scale":
+                sr = list(v) + [0] * 32
+                for i in range(32):
+                    o.slab_scale[i] = sr[i]
             else:
                 setattr(o, k, int(v))
         r = ProofReport()

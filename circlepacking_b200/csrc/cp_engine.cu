@@ -962,6 +962,13 @@ cp_status cp_proof_defaults(int family, cp_proof_opts* o) {
         o->geometric = 1;
         o->max_depth = 30;
         o->level_capacity = (int64_t)1 << 24;
+        // per slab, a coarse radius lattice that still proves it (r1 subdivisions
+        // out of the reference's 256; measured on B200: one step coarser left
+        // boxes unresolved or cost more boxes); the needed resolution grows
+        // toward lambda = 0.99
+        static const int32_t scale[18] = {128, 128, 128, 128, 128, 128, 128, 128, 128,
+                                          128, 144, 160, 176, 176, 192, 208, 224, 224};
+        for (int k = 0; k < 18; ++k) o->slab_scale[k] = scale[k];
     }
     return CP_OK;
 }
@@ -984,6 +991,10 @@ cp_status cp_prove_family(cp_prover* p, const cp_proof_opts* o, cp_proof_report*
         ro.policy = o->policy;
         ro.max_depth = o->max_depth;
         for (int d = 0; d < 4; ++d) ro.seed_sizes[d] = o->seed_sizes[d] > 0 ? o->seed_sizes[d] : 1;
+        if (k < 32 && o->slab_scale[k] > 0) {
+            for (int d = 1; d < 4; ++d)
+                ro.seed_sizes[d] = (int32_t)std::max<int64_t>(1, (int64_t)ro.seed_sizes[d] * o->slab_scale[k] / 256);
+        }
         ro.seed_lambda[0] = proof_slab_cut(*o, k);
         ro.seed_lambda[1] = proof_slab_cut(*o, k + 1);
         ro.level_capacity = o->level_capacity > 0 ? o->level_capacity : ((int64_t)1 << 24);

@@ -69,3 +69,22 @@ def test_prove_family_slabs_add_up(cp, prover):
         tot_dig = [(tot_dig[0] + r["digest"][0]) % (1 << 64), tot_dig[1] ^ r["digest"][1]]
         lo = hi
     assert got["evaluated"] == tot_eval and list(got["digest"]) == tot_dig
+
+
+def test_slab_scale_scales_each_slab_lattice(cp, prover):
+    """cp_proof_opts.slab_scale: slab k scales the radius subdivisions of the
+    seed by slab_scale[k] / 256 (here 128: [16, 16, 16, 4] in slab 0; 256: the
+    given [16, 32, 32, 8] in slab 1); the proof reports the sums of the two slab
+    refinements."""
+    family = cp.END_3D
+    got = prover.prove_family(family, slabs=2, geometric=1, seed_sizes=[16, 32, 32, 8], slab_scale=[128, 256],
+                              max_depth=16, digest=1)
+    assert got["slabs_done"] == 2
+    mid = 1.0 - (1.0 - cp.LAMBDA_MIN) * (((1.0 - cp.LAMBDA_MAX) / (1.0 - cp.LAMBDA_MIN)) ** 0.5)
+    tot_eval, tot_dig = 0, [0, 0]
+    for lam, sizes in (((cp.LAMBDA_MIN, mid), [16, 16, 16, 4]), ((mid, cp.LAMBDA_MAX), [16, 32, 32, 8])):
+        r = prover.refine(family, policy=cp.SPLIT_LAMBDA, max_depth=16, seed_sizes=sizes, seed_lambda=lam,
+                          level_capacity=1 << 23, engine=cp.ENGINE_GRAPH, digest=True)
+        tot_eval += r["evaluated"]
+        tot_dig = [(tot_dig[0] + r["digest"][0]) % (1 << 64), tot_dig[1] ^ r["digest"][1]]
+    assert got["evaluated"] == tot_eval and list(got["digest"]) == tot_dig
