@@ -276,20 +276,16 @@ def proof_leg(prover, cp, forms, families, world=1):
     run_kernel.cuh:110-127).  A family is proved when no box is left
     unresolved.  The best form runs every slab as one graph launch, the plain
     form as the FP64 host-driven level loop; both evaluate the same tree, which
-    the per-box verdict digests confirm.  The best form lets a child whose
-    radii are its parent's take the parent's lambda-independent terms (start
-    family, cp_refine_opts.reuse); the plain form recomputes them."""
+    the per-box verdict digests confirm."""
     out = []
     for f in families:
         prover.set_level_variant(f, cp.FP64, 0)
         # each rank refines its interleaved piece of every slab's lattice
         best_kw = dict(engine=cp.ENGINE_GRAPH, precision=forms[f]["precision"], digest=1, seed_parts=PARTS,
                        seed_part=PART)
-        # the plain form recomputes every criterion term of every box (no reuse of
-        # a parent's lambda-independent terms)
         plain_kw = dict(best_kw, engine=cp.ENGINE_LEVELS, precision=cp.FP64, reuse=0)
         # warm-up (graph build): one slab of a 4^dims seed as given, no per-slab scaling
-        prover.prove_family(f, **dict(best_kw, slabs=1, seed_sizes=[4, 4, 4, 4], slab_scale=[0] * 32))
+        prover.prove_family(f, **dict(best_kw, slabs=1, seed_sizes=[4, 4, 4, 4], slab_radii=[]))
         b = prover.prove_family(f, **best_kw)
         p = prover.prove_family(f, **plain_kw)
         same = (b["digest"] == p["digest"] and b["verdicts"] == p["verdicts"] and b["per_depth"] == p["per_depth"]

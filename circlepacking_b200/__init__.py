@@ -228,11 +228,12 @@ class ProofOpts(ctypes.Structure):
                 ("policy", ctypes.c_int32), ("max_depth", ctypes.c_int32), ("slabs", ctypes.c_int32),
                 ("geometric", ctypes.c_int32), ("seed_sizes", ctypes.c_int32 * 4), ("level_capacity", ctypes.c_int64),
                 ("digest", ctypes.c_int32), ("seed_parts", ctypes.c_int32), ("seed_part", ctypes.c_int32),
-                ("reuse", ctypes.c_int32), ("slab_scale", ctypes.c_int32 * 32)]
+                ("reuse", ctypes.c_int32), ("slab_radii", (ctypes.c_int32 * 3) * 32)]
 
     def as_dict(self) -> dict:
-        return {k: (list(getattr(self, k)) if k in ("seed_sizes", "slab_scale") else getattr(self, k))
-                for k, _ in self._fields_}
+        d = {k: (list(getattr(self, k)) if k == "seed_sizes" else getattr(self, k)) for k, _ in self._fields_}
+        d["slab_radii"] = [list(r) for r in self.slab_radii]
+        return d
 
 
 class ProofReport(ctypes.Structure):
@@ -462,10 +463,11 @@ class Prover:
                 ss = list(v) + [1] * 4
                 for d in range(4):
                     o.seed_sizes[d] = ss[d]
-            elif k == "slab_scale":
-                sr = list(v) + [0] * 32
+            elif k == "slab_radii":
+                rows = [list(r) for r in v] + [[0, 0, 0]] * 32
                 for i in range(32):
-                    o.slab_scale[i] = sr[i]
+                    for d in range(3):
+                        o.slab_radii[i][d] = rows[i][d]
             else:
                 setattr(o, k, int(v))
         r = ProofReport()

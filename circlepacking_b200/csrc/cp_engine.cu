@@ -950,25 +950,31 @@ cp_status cp_proof_defaults(int family, cp_proof_opts* o) {
     o->slabs = 1;
     o->geometric = 0;
     o->level_capacity = (int64_t)1 << 23;
-    o->reuse = 1;
-    // the radius resolution each family's lambda-only proof needs, with 64
-    // lambda cells over the whole range; start: geometric lambda slabs with the
-    // reference's own radius lattice per slab (start_configuration.cu:41-44)
+    // with the coarse seeds below, carrying a parent's lambda-independent terms
+    // costs more than it saves (measured on the start proof: 146 against 138 ms)
+    o->reuse = 0;
+    // the coarsest seed lattice that still proves each family with lambda-only
+    // refinement, found by a coordinate-descent search on B200 (each step
+    // coarsened one axis while the proof stayed complete with fewer boxes);
+    // start: geometric lambda slabs with a radius lattice per slab (below)
     static const int32_t seeds[6][4] = {{1, 256, 256, 64}, {64, 32, 32, 1},  {64, 64, 64, 16},
-                                        {64, 32, 32, 8},   {64, 128, 128, 1}, {64, 32, 32, 8}};
+                                        {51, 26, 21, 1},   {33, 66, 53, 1},   {41, 17, 17, 4}};
     for (int d = 0; d < 4; ++d) o->seed_sizes[d] = seeds[family][d];
     if (family == CP_START) {
         o->slabs = 18;
         o->geometric = 1;
         o->max_depth = 30;
         o->level_capacity = (int64_t)1 << 24;
-        // per slab, a coarse radius lattice that still proves it (r1 subdivisions
-        // out of the reference's 256; measured on B200: one step coarser left
-        // boxes unresolved or cost more boxes); the needed resolution grows
-        // toward lambda = 0.99
-        static const int32_t scale[18] = {128, 128, 128, 128, 128, 128, 128, 128, 128,
-                                          128, 144, 160, 176, 176, 192, 208, 224, 224};
-        for (int k = 0; k < 18; ++k) o->slab_scale[k] = scale[k];
+        // per slab, the coarsest radius lattice that still proves it, found by a
+        // coordinate-descent search on B200 (each step coarsened one radius axis
+        // while the slab stayed proved with fewer boxes).  r3 needs no
+        // subdivision at all; r1 needs the most, growing toward lambda = 0.99.
+        static const int32_t radii[18][3] = {
+            {30, 17, 1},   {37, 20, 1},   {41, 27, 1},   {51, 30, 1},   {60, 41, 1},   {67, 57, 1},
+            {79, 67, 1},   {93, 71, 1},   {109, 79, 1},  {128, 86, 1},  {144, 96, 1},  {160, 107, 1},
+            {176, 118, 1}, {176, 176, 1}, {192, 192, 1}, {208, 177, 1}, {224, 171, 1}, {224, 224, 1}};
+        for (int k = 0; k < 18; ++k)
+            for (int d = 0; d < 3; ++d) o->slab_radii[k][d] = radii[k][d];
     }
     return CP_OK;
 }
@@ -991,10 +997,9 @@ cp_status cp_prove_family(cp_prover* p, const cp_proof_opts* o, cp_proof_report*
         ro.policy = o->policy;
         ro.max_depth = o->max_depth;
         for (int d = 0; d < 4; ++d) ro.seed_sizes[d] = o->seed_sizes[d] > 0 ? o->seed_sizes[d] : 1;
-        if (k < 32 && o->slab_scale[k] > 0) {
+        if (k < 32)
             for (int d = 1; d < 4; ++d)
-                ro.seed_sizes[d] = (int32_t)std::max<int64_t>(1, (int64_t)ro.seed_sizes[d] * o->slab_scale[k] / 256);
-        }
+                if (o->slab_radii[k][d - 1] > 0) ro.seed_sizes[d] = o->slab_radii[k][d - 1];
         ro.seed_lambda[0] = proof_slab_cut(*o, k);
         ro.seed_lambda[1] = proof_slab_cut(*o, k + 1);
         ro.level_capacity = o->level_capacity > 0 ? o->level_capacity : ((int64_t)1 << 24);

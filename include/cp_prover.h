@@ -276,10 +276,9 @@ typedef struct cp_proof_opts {
     int32_t digest;          /* 1 = per-box verdict digest in the report */
     int32_t seed_parts;      /* > 1: refine only the interleaved piece seed_part of every slab's lattice */
     int32_t seed_part;       /* (one rank's share of the proof, see cp_refine_opts) */
-    int32_t reuse;           /* see cp_refine_opts.reuse (cp_proof_defaults: 1) */
-    int32_t slab_scale[32];  /* > 0: slab k (k < 32) scales the radius subdivisions of its seed by
-                                slab_scale[k] / 256: seed_sizes[d] * slab_scale[k] / 256 for d >= 1, at
-                                least 1; 0 = seed_sizes as given */
+    int32_t reuse;           /* see cp_refine_opts.reuse (cp_proof_defaults: 0) */
+    int32_t slab_radii[32][3]; /* slab k (k < 32): subdivisions of r1, r2, r3 of its seed lattice where
+                                  > 0, else seed_sizes[1..3] */
 } cp_proof_opts;
 
 typedef struct cp_proof_report {

@@ -88,13 +88,15 @@ def test_proof_defaults_without_device(libpath):
     d = o.as_dict()
     assert d["slabs"] == 18 and d["geometric"] == 1 and d["seed_sizes"] == [1, 256, 256, 64]
     assert d["policy"] == 1 and d["engine"] == 1  # lambda-only split, graph engine
-    # start: a radius lattice per slab, coarse at small lambda, finer toward 0.99
-    sr = d["slab_scale"]
-    assert all(0 < r <= 256 for r in sr[:18]) and sr[18:] == [0] * 14
-    assert sr[:18] == sorted(sr[:18]) and d["reuse"] == 1
+    # start: a radius lattice per slab; r1 the finest axis, growing toward lambda = 0.99
+    sr = d["slab_radii"]
+    assert all(0 < r[0] <= 256 and 0 < r[1] <= r[0] and r[2] >= 1 for r in sr[:18])
+    assert sr[18:] == [[0, 0, 0]] * 14
+    r1 = [r[0] for r in sr[:18]]
+    assert r1 == sorted(r1)
     for f in range(1, 6):
         assert L.cp_proof_defaults(f, ctypes.byref(o)) == 0
-        assert o.slabs == 1 and o.seed_sizes[0] == 64 and o.max_depth == 24
-        assert list(o.slab_scale) == [0] * 32
+        assert o.slabs == 1 and o.seed_sizes[0] >= 32 and o.max_depth == 24
+        assert all(list(r) == [0, 0, 0] for r in o.slab_radii)
     L.cp_prove_family.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     assert L.cp_prove_family(None, None, None) == 1

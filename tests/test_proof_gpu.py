@@ -1,13 +1,14 @@
-"""Full-domain proofs on the GPU: five of the six families (all but start) are
-proved over their whole domain (lambda in [0.5, 0.99] and the dependent radius
-ranges) by lambda-only bisection -- the reference's own refinement rule, applied
-per box -- from a lattice seed with 64 lambda slabs and the radius resolution
-each family needs.  Both engines evaluate the same tree of boxes."""
+"""Full-domain proofs on the GPU: the families other than start are proved over
+their whole domain (lambda in [0.5, 0.99] and the dependent radius ranges) by
+lambda-only bisection -- the reference's own refinement rule, applied per box --
+from one lattice seed over the whole lambda range with the resolution the
+family needs (start, proved by lambda slabs, has its own test at the end).
+Both engines evaluate the same tree of boxes."""
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-SEEDS = {1: (64, 32, 32), 2: (64, 64, 64, 16), 3: (64, 32, 32, 8), 4: (64, 128, 128), 5: (64, 32, 32, 8)}
+SEEDS = {1: (64, 32, 32), 2: (64, 64, 64, 16), 3: (51, 26, 21, 1), 4: (33, 66, 53), 5: (41, 17, 17, 4)}
 
 
 @pytest.fixture(scope="module")
@@ -35,9 +36,9 @@ def test_family_proved_over_full_domain(cp, prover, family):
 @pytest.mark.parametrize("family", [1, 3, 5])
 def test_prove_family_driver_matches_refinement(cp, prover, family):
     """cp_prove_family with the library's defaults for a family runs the same
-    refinement as the explicit cp_refine call above (one slab of 64 lambda
-    cells), box for box: same counts and the same per-box verdict digest in
-    both engines."""
+    refinement as the explicit cp_refine call above (one slab, the family's
+    seed lattice), box for box: same counts and the same per-box verdict digest
+    in both engines."""
     d = prover.proof_defaults(family)
     assert d["slabs"] == 1 and d["policy"] == cp.SPLIT_LAMBDA
     assert tuple(d["seed_sizes"][:cp.DIMS[family]]) == SEEDS[family]
@@ -71,13 +72,12 @@ def test_prove_family_slabs_add_up(cp, prover):
     assert got["evaluated"] == tot_eval and list(got["digest"]) == tot_dig
 
 
-def test_slab_scale_scales_each_slab_lattice(cp, prover):
-    """cp_proof_opts.slab_scale: slab k scales the radius subdivisions of the
-    seed by slab_scale[k] / 256 (here 128: [16, 16, 16, 4] in slab 0; 256: the
-    given [16, 32, 32, 8] in slab 1); the proof reports the sums of the two slab
-    refinements."""
+def test_slab_radii_set_each_slab_lattice(cp, prover):
+    """cp_proof_opts.slab_radii: slab k seeds its own r1 x r2 x r3 subdivisions
+    where given (here [16, 16, 4] in slab 0; slab 1 keeps seed_sizes); the proof
+    reports the sums of the two slab refinements."""
     family = cp.END_3D
-    got = prover.prove_family(family, slabs=2, geometric=1, seed_sizes=[16, 32, 32, 8], slab_scale=[128, 256],
+    got = prover.prove_family(family, slabs=2, geometric=1, seed_sizes=[16, 32, 32, 8], slab_radii=[[16, 16, 4]],
                               max_depth=16, digest=1)
     assert got["slabs_done"] == 2
     mid = 1.0 - (1.0 - cp.LAMBDA_MIN) * (((1.0 - cp.LAMBDA_MAX) / (1.0 - cp.LAMBDA_MIN)) ** 0.5)
@@ -88,3 +88,17 @@ def test_slab_scale_scales_each_slab_lattice(cp, prover):
         tot_eval += r["evaluated"]
         tot_dig = [(tot_dig[0] + r["digest"][0]) % (1 << 64), tot_dig[1] ^ r["digest"][1]]
     assert got["evaluated"] == tot_eval and list(got["digest"]) == tot_dig
+
+
+def test_start_proved_over_full_domain(cp, prover):
+    """The start family's proof with the library's defaults (18 geometric lambda
+    slabs, a radius lattice per slab): every box proved, empty or clipped, in
+    both engines, with and without reuse of the parents' lambda-independent
+    terms, and the four runs evaluate the same boxes with the same verdicts."""
+    runs = [prover.prove_family(cp.START, engine=e, reuse=u, digest=1)
+            for e in (cp.ENGINE_GRAPH, cp.ENGINE_LEVELS) for u in (0, 1)]
+    for r in runs:
+        assert r["proved"] and r["unresolved"] == 0 and r["slabs_done"] == 18
+        for k in ("evaluated", "verdicts", "clipped", "per_depth", "digest"):
+            assert r[k] == runs[0][k], k
+    assert runs[0]["verdicts"][1] > 0  # boxes were critical at coarser levels and got refined
