@@ -121,6 +121,7 @@ extern "C" cp_status cp_refine_boxes_static(int family, int precision, int polic
         lv[l].hi = lv[l].lo + (size_t)D * cap;
         lv[l].depth = (uint8_t*)(lv[l].hi + (size_t)D * cap);
         lv[l].cap = cap;
+        lv[l].aux = nullptr;  // no lambda-independent terms in the fixed scratch
         cnt_in[l] = 0;
         p += bytes;
     }

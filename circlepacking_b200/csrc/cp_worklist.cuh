@@ -15,7 +15,7 @@ struct BoxList {
     double* hi;
     uint8_t* depth;
     size_t cap;
-    double* aux;
+    double* aux = nullptr;  // a list built member by member carries no terms
 };
 constexpr int kAuxFields = 4;
 
