@@ -630,28 +630,37 @@ def main():
         h2d = sum(int(seeds[f][0].numel() * 8 * 2 + seeds[f][2].numel()) for f in FAMILIES)
         d2h = len(FAMILIES) * __import__("ctypes").sizeof(cp.RefineReport)
 
-        def e2e_step():
+        def stage(k, f):
+            lo, hi, dp = seeds[f]
+            prover.stage_boxes(k % 2, lo.numpy(), hi.numpy(), dp.numpy())
+
+        def e2e_steps(steps):
+            """`steps` steps of the host-buffer path: every family's seeds are copied
+            from pinned host memory into a staging slot while the previous family
+            refines (cp_stage_boxes_host / cp_refine_staged, two slots); each report
+            comes back to the host."""
+            jobs = [f for _ in range(steps) for f in FAMILIES]
             tot = 0
-            for f in FAMILIES:
-                lo, hi, dp = seeds[f]
-                r = prover.refine_boxes(f, lo.numpy(), hi.numpy(), depth=dp.numpy(),
-                                        **{k: v for k, v in seed_opts(f, forms[f], args.depth).items()
-                                           if k not in ("seed_sizes", "seed_lambda")})
+            stage(0, jobs[0])
+            for k, f in enumerate(jobs):
+                if k + 1 < len(jobs):
+                    stage(k + 1, jobs[k + 1])
+                r = prover.refine_staged(f, k % 2, **{kk: v for kk, v in seed_opts(f, forms[f], args.depth).items()
+                                                      if kk not in ("seed_sizes", "seed_lambda")})
                 tot += r["evaluated"]
             return tot
 
-        e2e_step()
+        e2e_steps(1)
         torch.cuda.synchronize()
         barrier(world)
         t0 = time.perf_counter()
-        tot = 0
-        for _ in range(args.steps):
-            tot += e2e_step()
+        tot = e2e_steps(args.steps)
         torch.cuda.synchronize()
         dt = max_over_ranks(world, (time.perf_counter() - t0) / args.steps)
         e2e = {"value": sum_over_ranks(world, tot / args.steps) / dt, "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3,
-               "call": "cp_refine_boxes_host per family (host seed boxes, report back), best form"}
+               "call": "cp_stage_boxes_host + cp_refine_staged per family (host seed boxes copied while the "
+                       "previous family refines, report back), best form"}
 
     log("e2e done")
     # ---- the FP32 pre-pass form of the whole step, and the uneven-depth worklist

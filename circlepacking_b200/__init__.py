@@ -261,6 +261,8 @@ def _declare_handle(L):
     L.cp_refine.argtypes = [P, ctypes.POINTER(RefineOpts), ctypes.POINTER(RefineReport)]
     L.cp_refine_boxes.argtypes = [P, ctypes.POINTER(RefineOpts), P, P, P, SZ, ctypes.POINTER(RefineReport)]
     L.cp_refine_boxes_host.argtypes = [P, ctypes.POINTER(RefineOpts), P, P, P, SZ, ctypes.POINTER(RefineReport)]
+    L.cp_stage_boxes_host.argtypes = [P, I, P, P, P, SZ, I]
+    L.cp_refine_staged.argtypes = [P, ctypes.POINTER(RefineOpts), I, ctypes.POINTER(RefineReport)]
     L.cp_reference_step.argtypes = [P, I, D, D, P, P, P]
     L.cp_prove_family_reference.argtypes = [P, I, D, D, P, I64, P, ctypes.POINTER(ReferenceReport)]
     L.cp_reference_criticals.argtypes = [P, I, D, D, P, SZ, P, P, ctypes.POINTER(SZ)]
@@ -412,6 +414,30 @@ class Prover:
         o = self.opts(family, **kw)
         r = RefineReport()
         _check(self._L.cp_refine(self._h, ctypes.byref(o), ctypes.byref(r)), "cp_refine")
+        return r.as_dict()
+
+    def stage_boxes(self, slot, lo, hi, depth=None):
+        """Starts the host-to-device copy of seed boxes (numpy [dims][n]; page-locked
+        memory, e.g. a pinned torch tensor's numpy view, for the copy to overlap)
+        into staging slot 0 or 1 (cp_stage_boxes_host) and returns at once.  The
+        arrays are kept alive until refine_staged(slot) returns."""
+        lo = np.ascontiguousarray(lo, np.float64)
+        hi = np.ascontiguousarray(hi, np.float64)
+        dp = np.ascontiguousarray(depth, np.uint8) if depth is not None else None
+        staged = self.__dict__.setdefault("_staged", [None, None])
+        staged[slot] = (lo, hi, dp)
+        _check(self._L.cp_stage_boxes_host(self._h, slot, lo.ctypes.data, hi.ctypes.data,
+                                           dp.ctypes.data if dp is not None else None, lo.shape[1], lo.shape[0]),
+               "cp_stage_boxes_host")
+
+    def refine_staged(self, family, slot, **kw) -> dict:
+        """Refines the boxes staged in a slot (cp_refine_staged); same report as refine_boxes."""
+        o = self.opts(family, **kw)
+        r = RefineReport()
+        try:
+            _check(self._L.cp_refine_staged(self._h, ctypes.byref(o), slot, ctypes.byref(r)), "cp_refine_staged")
+        finally:
+            self.__dict__.setdefault("_staged", [None, None])[slot] = None
         return r.as_dict()
 
     def refine_boxes(self, family, lo, hi, depth=None, **kw) -> dict:

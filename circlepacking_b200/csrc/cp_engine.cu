@@ -86,6 +86,23 @@ __global__ void k_copy_seed(int dims, const double* __restrict__ lo, const doubl
     }
 }
 
+__global__ void k_set_u64(unsigned long long* p, unsigned long long v) { *p = v; }
+__global__ void k_zero_u64(unsigned long long* p, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 0;
+}
+
+// The graph engine's level table and schedule, passed by value (about 3 KB of
+// kernel parameters).
+struct GraphUpload {
+    BoxList levels[kMaxLevels];
+    DevSched sched;
+    int nlevels;
+};
+__global__ void k_graph_upload(GraphUpload u, BoxList* levels, DevSched* sched) {
+    for (int l = threadIdx.x; l < u.nlevels; l += blockDim.x) levels[l] = u.levels[l];
+    if (threadIdx.x == 0) *sched = u.sched;
+}
+
 // Seeded random boxes on the family's domain (the uneven-depth workload of the
 // persistent engine).  Box i draws its numbers from a counter-based generator:
 // u(i, k) = top 53 bits of mix64(seed ^ mix64(8 i + k)) / 2^53.  Lambda has its
@@ -326,6 +343,15 @@ struct cp_prover {
     // called after every chunk of a host-driven refinement
     cp_chunk_callback chunk_cb = nullptr;
     void* chunk_user = nullptr;
+    // host seeds staged on a copy stream (cp_stage_boxes_host / cp_refine_staged)
+    cudaStream_t copy_stream = nullptr;
+    struct Stage {
+        unsigned char* buf = nullptr;  // lo [dims][n] doubles, hi [dims][n] doubles, depth [n] bytes
+        size_t bytes = 0, n = 0;
+        int dims = 0;
+        bool has_depth = false, staged = false;
+        cudaEvent_t done = nullptr;  // the copy has landed
+    } stage[2];
 };
 
 cudaStream_t cp_prover_stream(cp_prover* p) { return p->stream; }
@@ -343,9 +369,11 @@ cp_status cuda_ok(cudaError_t e, cp_status s = CP_ERR_CUDA) {
         if (s_ != CP_OK) return s_;    \
     } while (0)
 
+// Zeroes the counters and per-depth bins with a kernel: a memset may run on a
+// copy engine and wait there behind a large host-to-device copy of staged seeds.
 cp_status reset_counters(cp_prover* p) {
-    CP_TRY(cuda_ok(cudaMemsetAsync(p->cnt, 0, sizeof(unsigned long long) * C_COUNT, p->stream)));
-    return cuda_ok(cudaMemsetAsync(p->per_depth, 0, sizeof(unsigned long long) * kDepthBins, p->stream));
+    k_zero_u64<<<1, 128, 0, p->stream>>>(p->cnt, (int)(C_COUNT + kDepthBins));
+    return cp_check_launch();
 }
 
 cp_status read_counters(cp_prover* p) {
@@ -513,7 +541,8 @@ cp_status cp_engine_eval_chunk(cp_prover* p, int fam, const cp_refine_opts& o, L
     a.digest = o.digest ? 1 : 0;
     // children append after the boxes already in `out`
     unsigned long long base = out ? out->n : 0;
-    CP_TRY(cuda_ok(cudaMemcpyAsync(p->cnt + C_OUT, &base, sizeof(base), cudaMemcpyHostToDevice, p->stream)));
+    k_set_u64<<<1, 1, 0, p->stream>>>(p->cnt + C_OUT, base);
+    CP_TRY(cp_check_launch());
     LevelKernel k = level_kernel(fam, o.precision, p->variant[fam][o.precision ? 1 : 0]);
     const int block = kEvalBlock;
     unsigned grid = grid_of(k, block);
@@ -728,8 +757,17 @@ cp_status refine_graph(cp_prover* p, const cp_refine_opts& o, cp_refine_report* 
     hs.nlevels = nlevels;
     hs.max_depth = o.max_depth;
     hs.fanout = fanout(o.policy == CP_SPLIT_LEARNED ? SPLIT_GIVEN : o.policy, D);
-    CP_TRY(cuda_ok(cudaMemcpyAsync(p->d_levels, hl, sizeof(BoxList) * nlevels, cudaMemcpyHostToDevice, p->stream)));
-    CP_TRY(cuda_ok(cudaMemcpyAsync(p->d_sched, &hs, sizeof(DevSched), cudaMemcpyHostToDevice, p->stream)));
+    {
+        // the level table and the schedule travel as kernel parameters: a copy
+        // would queue behind a large host-to-device copy of staged seeds on the
+        // copy engine and delay the refinement
+        GraphUpload u;
+        for (int l = 0; l < nlevels; ++l) u.levels[l] = hl[l];
+        u.sched = hs;
+        u.nlevels = nlevels;
+        k_graph_upload<<<1, 64, 0, p->stream>>>(u, p->d_levels, p->d_sched);
+        CP_TRY(cp_check_launch());
+    }
     double ls = lambda_scale_of(o);
     unsigned long long ls_bits;
     std::memcpy(&ls_bits, &ls, 8);
@@ -874,6 +912,12 @@ void cp_destroy(cp_prover* p) {
     cudaFree(p->slab_single);
     if (p->ev0) cudaEventDestroy(p->ev0);
     if (p->ev1) cudaEventDestroy(p->ev1);
+    if (p->copy_stream) cudaStreamSynchronize(p->copy_stream);
+    for (auto& st : p->stage) {
+        cudaFree(st.buf);
+        if (st.done) cudaEventDestroy(st.done);
+    }
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;
 }
@@ -1164,6 +1208,72 @@ cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* o, const doub
             CP_TRY(cuda_ok(cudaMemcpyAsync(b.depth, depth, n, cudaMemcpyHostToDevice, p->stream)));
         else
             CP_TRY(cuda_ok(cudaMemsetAsync(b.depth, 0, n, p->stream)));
+    }
+    p->levels[0].n = n;
+    CP_TRY(reset_counters(p));
+    return run_refinement(p, *o, r, t0);
+}
+
+cp_status cp_stage_boxes_host(cp_prover* p, int slot, const double* lo, const double* hi, const uint8_t* depth,
+                              size_t n, int dims) {
+    if (!p || slot < 0 || slot > 1 || (dims != 3 && dims != 4) || (n && (!lo || !hi))) return CP_ERR_INVALID;
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    if (!p->copy_stream) CP_TRY(cuda_ok(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking)));
+    cp_prover::Stage& st = p->stage[slot];
+    if (!st.done) CP_TRY(cuda_ok(cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming)));
+    const size_t axis = sizeof(double) * (size_t)dims * n;
+    const size_t need = 2 * axis + n;
+    if (st.bytes < need) {
+        // the slot's previous copy and any refinement reading it have finished
+        // (the refinement is synchronous), so the buffer can be replaced
+        CP_TRY(cuda_ok(cudaStreamSynchronize(p->copy_stream)));
+        cudaFree(st.buf);
+        st.buf = nullptr;
+        st.bytes = 0;
+        CP_TRY(cuda_ok(cudaMalloc(&st.buf, need)));
+        st.bytes = need;
+    }
+    st.n = n;
+    st.dims = dims;
+    st.has_depth = depth != nullptr;
+    if (n) {
+        CP_TRY(cuda_ok(cudaMemcpyAsync(st.buf, lo, axis, cudaMemcpyHostToDevice, p->copy_stream)));
+        CP_TRY(cuda_ok(cudaMemcpyAsync(st.buf + axis, hi, axis, cudaMemcpyHostToDevice, p->copy_stream)));
+        if (depth) CP_TRY(cuda_ok(cudaMemcpyAsync(st.buf + 2 * axis, depth, n, cudaMemcpyHostToDevice, p->copy_stream)));
+    }
+    CP_TRY(cuda_ok(cudaEventRecord(st.done, p->copy_stream)));
+    st.staged = true;
+    return CP_OK;
+}
+
+cp_status cp_refine_staged(cp_prover* p, const cp_refine_opts* o, int slot, cp_refine_report* r) {
+    if (!p || !r || slot < 0 || slot > 1) return CP_ERR_INVALID;
+    CP_TRY(check_opts(o));
+    cp_prover::Stage& st = p->stage[slot];
+    if (!st.staged) return cp_fail(CP_ERR_INVALID, "cp_refine_staged: slot %d holds no staged boxes", slot);
+    const int D = family_dims(o->family);
+    if (st.dims != D) return cp_fail(CP_ERR_INVALID, "cp_refine_staged: slot %d holds %d-axis boxes", slot, st.dims);
+    p->pending = false;
+    p->interrupt.store(0);
+    const double t0 = now_ms();
+    std::memset(r, 0, sizeof(*r));
+    CP_TRY(cuda_ok(cudaSetDevice(p->device)));
+    const size_t n = st.n;
+    const size_t cap = o->level_capacity > 0 ? (size_t)o->level_capacity : ((size_t)1 << 25);
+    if (n > cap) return CP_ERR_CAPACITY;
+    CP_TRY(ensure_levels(p, o->max_depth + 1, D, cap));
+    for (auto& L : p->levels) L.n = 0;
+    // the refinement's stream waits for the slot's copy, then moves the boxes
+    // into the level stack (device to device)
+    CP_TRY(cuda_ok(cudaStreamWaitEvent(p->stream, st.done, 0)));
+    // (a kernel, not a device-to-device copy, which could queue on a copy
+    // engine behind the next slot's host-to-device copy)
+    const double* slo = reinterpret_cast<const double*>(st.buf);
+    const double* shi = slo + (size_t)D * n;
+    const uint8_t* sdp = st.has_depth ? st.buf + 2 * sizeof(double) * D * n : nullptr;
+    if (n) {
+        k_copy_seed<<<grid_of(k_copy_seed, 128), 128, 0, p->stream>>>(D, slo, shi, sdp, n, p->levels[0].b);
+        CP_TRY(cp_check_launch());
     }
     p->levels[0].n = n;
     CP_TRY(reset_counters(p));

@@ -363,6 +363,19 @@ cp_status cp_random_boxes(cp_prover* p, int family, uint64_t seed, int max_label
 cp_status cp_refine_boxes_host(cp_prover* p, const cp_refine_opts* opts, const double* lo, const double* hi,
                                const uint8_t* depth, size_t n, cp_refine_report* report);
 
+/* Host seeds through two staging slots, so that the copy of the next seed set
+ * overlaps the refinement of the current one.  cp_stage_boxes_host starts the
+ * host-to-device copy of n boxes of `dims` axes (lo/hi SoA with stride n;
+ * depth: n bytes or NULL for depth 0) into staging slot 0 or 1 on the handle's
+ * copy stream and returns at once; the host buffers must stay untouched until
+ * the refinement that uses the slot has returned, and must be page-locked for
+ * the copy to overlap.  cp_refine_staged refines the boxes of a slot as
+ * cp_refine_boxes_host would (same report), after the slot's copy finished.
+ * A slot may be staged again once the refinement that used it has returned. */
+cp_status cp_stage_boxes_host(cp_prover* p, int slot, const double* lo, const double* hi, const uint8_t* depth,
+                              size_t n, int dims);
+cp_status cp_refine_staged(cp_prover* p, const cp_refine_opts* opts, int slot, cp_refine_report* report);
+
 /* Diagnostics: the library's directed division (Newton reciprocal + exact
  * FMA remainders, used for every interval division in place of the
  * reference's __ddiv_rd/__ddiv_ru, interval.cuh:261-310) next to those

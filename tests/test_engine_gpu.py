@@ -155,3 +155,42 @@ def test_cpu_restated_refinement_matches_device(cp, oracle, family):
     for v in range(5):
         a, b = want["verdicts"][v], got["verdicts"][v]
         assert abs(a - b) <= 1e-3 * max(a, b) + 2, (v, a, b)
+
+
+def test_staged_host_seeds_match_host_entry(cp):
+    """cp_stage_boxes_host + cp_refine_staged give the report of
+    cp_refine_boxes_host, with the two slots alternating and the next slot's
+    copy in flight while a refinement runs."""
+    import torch
+
+    p = cp.Prover(0)
+    try:
+        sets = []
+        for f, sizes in ((cp.MIDDLE, [16, 8, 8, 4]), (cp.END_2D, [16, 16, 8]), (cp.START, [8, 8, 8, 4])):
+            lo, hi, vis = cp.lattice_boxes(f, (cp.LAMBDA_MIN, cp.LAMBDA_MAX), sizes,
+                                           np.arange(int(np.prod(sizes))), visited=True)
+            hlo = torch.empty(lo.shape, dtype=torch.float64, pin_memory=True)
+            hhi = torch.empty(hi.shape, dtype=torch.float64, pin_memory=True)
+            hdp = torch.empty(vis.shape, dtype=torch.uint8, pin_memory=True)
+            hlo.copy_(lo)
+            hhi.copy_(hi)
+            hdp.copy_(torch.where(vis != 0, 0, 255).to(torch.uint8))
+            sets.append((f, hlo.numpy(), hhi.numpy(), hdp.numpy()))
+        kw = dict(policy=cp.SPLIT_UNIFORM, max_depth=2, digest=True, engine=cp.ENGINE_GRAPH)
+        want = [p.refine_boxes(f, lo, hi, depth=dp, **kw) for f, lo, hi, dp in sets]
+        jobs = sets + sets
+        p.stage_boxes(0, *jobs[0][1:])
+        for k, (f, lo, hi, dp) in enumerate(jobs):
+            if k + 1 < len(jobs):
+                p.stage_boxes((k + 1) % 2, *jobs[k + 1][1:])
+            got = p.refine_staged(f, k % 2, **kw)
+            for key in ("evaluated", "verdicts", "unresolved", "clipped", "per_depth", "digest"):
+                assert got[key] == want[k % len(sets)][key], (k, key)
+        # a slot keeps its boxes on the device: refining it again gives the same report
+        k = len(jobs) - 1
+        again = p.refine_staged(jobs[k][0], k % 2, **kw)
+        assert again["digest"] == want[k % len(sets)]["digest"]
+        with pytest.raises(cp.ProverError):
+            p.refine_staged(cp.END_2D, k % 2, **kw)  # 4-axis boxes staged, 3-axis family
+    finally:
+        p.close()
