@@ -97,18 +97,21 @@ __device__ __forceinline__ void level_smem_init(LevelSmem<WARPS>& sm) {
 // warp's collective child write).  All 32 lanes of the warp must call it.
 // ord_in / axis_in >= 0: this box's criterion order / split axis (SPLIT_GIVEN),
 // from a network run inline; otherwise the hint arrays (or the defaults).
+template <int FAM, int WARPS>
+__device__ __forceinline__ void level_emit(const LevelArgs& a, LevelSmem<WARPS>& sm, int v, bool clipped,
+                                           bool fp32_decided, const double* lo, const double* hi, int depth,
+                                           int given, const LaFree& lf);
+
 template <int FAM, int PREC, int WARPS>
 __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSmem<WARPS>& sm, unsigned& handles,
                                            int ord_in = -1, int axis_in = -1) {
     constexpr int D = family_dims(FAM);
     const size_t i = a.begin + j;
-    unsigned nchild = 0;
-    double lo[4], hi[4];
-    int depth = 0, axis = 0;
+    double lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
+    int depth = 0, given = 0;
     int v = -1;                 // this lane's verdict (-1: no box evaluated)
     LaFree lf{0.0, 0.0, 0.0, 0.0};  // start family: the box's lambda-independent terms, when known
-    bool clipped = false, unresolved = false, fp32_decided = false;
-    unsigned long long h = 0;   // digest hash of (box, verdict)
+    bool clipped = false, fp32_decided = false;
     if (j < a.count) {
         depth = a.in.depth[i];
         if (depth == 0xFF) {
@@ -146,19 +149,39 @@ __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSm
                 v = r.verdict;
                 handles += r.handles;
             }
-            if (a.digest) h = box_hash<D>(lo, hi, v);
-            if (v != V_PROVED && v != V_EMPTY) {
-                if (depth >= a.max_depth) {
-                    unresolved = true;
-                } else {
-                    nchild = fanout(a.policy, D);
-                    if (a.policy == SPLIT_WIDEST)
-                        axis = widest_axis<D>(lo, hi);
-                    else if (a.policy == SPLIT_HYBRID)
-                        axis = hybrid_axis<D>(lo, hi, a.lambda_scale);
-                    else if (a.policy == SPLIT_GIVEN)
-                        axis = axis_in >= 0 ? axis_in % D : (a.axis_hint ? (a.axis_hint[j] % D) : 0);
-                }
+            if (a.policy == SPLIT_GIVEN) given = axis_in >= 0 ? axis_in % D : (a.axis_hint ? (a.axis_hint[j] % D) : 0);
+        }
+    }
+    level_emit<FAM>(a, sm, v, clipped, fp32_decided, lo, hi, depth, given, lf);
+}
+
+// The end of a level step, for every lane of a warp (all 32 must call it):
+// v = the lane's verdict (-1: no box evaluated), its box lo/hi and depth,
+// given = its split axis for SPLIT_GIVEN, lf = its lambda-independent terms.
+// Counts the verdicts, folds the digest and writes the children of every box
+// that is neither proved nor empty (unresolved at the depth limit).
+template <int FAM, int WARPS>
+__device__ __forceinline__ void level_emit(const LevelArgs& a, LevelSmem<WARPS>& sm, int v, bool clipped,
+                                           bool fp32_decided, const double* lo, const double* hi, int depth,
+                                           int given, const LaFree& lf) {
+    constexpr int D = family_dims(FAM);
+    unsigned nchild = 0;
+    int axis = 0;
+    bool unresolved = false;
+    unsigned long long h = 0;  // digest hash of (box, verdict)
+    if (v >= 0) {
+        if (a.digest) h = box_hash<D>(lo, hi, v);
+        if (v != V_PROVED && v != V_EMPTY) {
+            if (depth >= a.max_depth) {
+                unresolved = true;
+            } else {
+                nchild = fanout(a.policy, D);
+                if (a.policy == SPLIT_WIDEST)
+                    axis = widest_axis<D>(lo, hi);
+                else if (a.policy == SPLIT_HYBRID)
+                    axis = hybrid_axis<D>(lo, hi, a.lambda_scale);
+                else if (a.policy == SPLIT_GIVEN)
+                    axis = given;
             }
         }
     }
