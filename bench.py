@@ -258,10 +258,10 @@ def train_models(prover, cp, depth):
 
 # DRAM traffic of the graph refinement per evaluated box, from one ncu capture
 # (middle family, 32^4 seed, one level: 11.95M boxes evaluated, 10.9M children
-# written, 1.154 GB read + 1.237 GB written); algorithmic: 65 B read per 4-D box
+# written, 1.118 GB read + 1.208 GB written); algorithmic: 65 B read per 4-D box
 # and 65 B written per child.  FP64 pipe activity of the same capture.
-TRAFFIC_PER_BOX, ALGORITHMIC_BYTES_PER_BOX = 2.391e9 / 11.95e6, 124.0
-FP64_PIPE_ACTIVE_NCU = 0.209
+TRAFFIC_PER_BOX, ALGORITHMIC_BYTES_PER_BOX = 2.326e9 / 11.95e6, 124.0
+FP64_PIPE_ACTIVE_NCU = 0.239
 
 PROOF_FAMILIES = (0, 1, 2, 3, 4, 5)
 
