@@ -1019,6 +1019,18 @@ cp_status cp_proof_defaults(int family, cp_proof_opts* o) {
             {176, 118, 1}, {176, 176, 1}, {192, 192, 1}, {208, 177, 1}, {224, 171, 1}, {224, 224, 1}};
         for (int k = 0; k < 18; ++k)
             for (int d = 0; d < 3; ++d) o->slab_radii[k][d] = radii[k][d];
+    } else if (family == CP_START_END_3D) {
+        // the same geometric slabs, each with its searched radius lattice:
+        // 1.30e8 boxes against 2.26e8 for one 64 x 64 x 64 x 16 seed
+        o->slabs = 18;
+        o->geometric = 1;
+        o->seed_sizes[0] = 1;
+        static const int32_t radii[18][3] = {
+            {26, 41, 8},  {26, 26, 10}, {33, 26, 10}, {33, 33, 10}, {33, 33, 10}, {41, 33, 10},
+            {41, 33, 10}, {33, 41, 10}, {41, 41, 10}, {41, 41, 10}, {41, 51, 10}, {41, 51, 10},
+            {51, 51, 10}, {51, 51, 10}, {51, 51, 10}, {51, 51, 10}, {51, 51, 10}, {51, 51, 10}};
+        for (int k = 0; k < 18; ++k)
+            for (int d = 0; d < 3; ++d) o->slab_radii[k][d] = radii[k][d];
     }
     return CP_OK;
 }

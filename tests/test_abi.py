@@ -94,9 +94,13 @@ def test_proof_defaults_without_device(libpath):
     assert sr[18:] == [[0, 0, 0]] * 14
     r1 = [r[0] for r in sr[:18]]
     assert r1 == sorted(r1)
-    for f in range(1, 6):
+    for f in (1, 3, 4, 5):
         assert L.cp_proof_defaults(f, ctypes.byref(o)) == 0
         assert o.slabs == 1 and o.seed_sizes[0] >= 32 and o.max_depth == 24
         assert all(list(r) == [0, 0, 0] for r in o.slab_radii)
+    # start_end_3d: the start proof's geometric slabs, a radius lattice per slab
+    assert L.cp_proof_defaults(2, ctypes.byref(o)) == 0
+    assert o.slabs == 18 and o.geometric == 1 and o.seed_sizes[0] == 1
+    assert all(r[0] > 0 and r[1] > 0 and r[2] > 0 for r in o.slab_radii[:18])
     L.cp_prove_family.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     assert L.cp_prove_family(None, None, None) == 1

@@ -102,3 +102,14 @@ def test_start_proved_over_full_domain(cp, prover):
         for k in ("evaluated", "verdicts", "clipped", "per_depth", "digest"):
             assert r[k] == runs[0][k], k
     assert runs[0]["verdicts"][1] > 0  # boxes were critical at coarser levels and got refined
+
+
+def test_start_end_3d_proved_by_slabs(cp, prover):
+    """start_end_3d's default proof (18 geometric lambda slabs, a radius
+    lattice per slab): proved in both engines, with the same boxes and
+    verdicts."""
+    runs = [prover.prove_family(cp.START_END_3D, engine=e, digest=1) for e in (cp.ENGINE_GRAPH, cp.ENGINE_LEVELS)]
+    for r in runs:
+        assert r["proved"] and r["unresolved"] == 0 and r["slabs_done"] == 18
+        for k in ("evaluated", "verdicts", "clipped", "per_depth", "digest"):
+            assert r[k] == runs[0][k], k
