@@ -1000,7 +1000,7 @@ cp_status cp_proof_defaults(int family, cp_proof_opts* o) {
     // the coarsest seed lattice that still proves each family with lambda-only
     // refinement, found by a coordinate-descent search on B200 (each step
     // coarsened one axis while the proof stayed complete with fewer boxes);
-    // start: geometric lambda slabs with a radius lattice per slab (below)
+    // start and start_end_3d: geometric lambda slabs with a radius lattice per slab (below)
     static const int32_t seeds[6][4] = {{1, 256, 256, 64}, {64, 32, 32, 1},  {64, 64, 64, 16},
                                         {51, 26, 21, 1},   {33, 66, 53, 1},   {41, 17, 17, 4}};
     for (int d = 0; d < 4; ++d) o->seed_sizes[d] = seeds[family][d];

@@ -295,8 +295,10 @@ typedef struct cp_proof_report {
     uint64_t digest[2];
 } cp_proof_report;
 
-/* The library's settings for a family's full-domain proof (the seeds its
- * refinement needs); CP_ERR_INVALID for a bad family. */
+/* The library's settings for a family's full-domain proof: lambda-only
+ * refinement from the coarsest seed lattice that proves the family (start and
+ * start_end_3d: 18 geometric lambda slabs with a radius lattice per slab),
+ * graph engine; CP_ERR_INVALID for a bad family. */
 cp_status cp_proof_defaults(int family, cp_proof_opts* opts);
 
 /* The proof of one family (opts->family).  Stops between slabs on
