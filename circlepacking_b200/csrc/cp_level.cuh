@@ -93,15 +93,16 @@ __device__ __forceinline__ void level_smem_init(LevelSmem<WARPS>& sm) {
     }
 }
 
-// One lane's box j of the chunk (j >= a.count: the lane only takes part in the
-// warp's collective child write).  All 32 lanes of the warp must call it.
-// ord_in / axis_in >= 0: this box's criterion order / split axis (SPLIT_GIVEN),
-// from a network run inline; otherwise the hint arrays (or the defaults).
+// (defined below)
 template <int FAM, int WARPS>
 __device__ __forceinline__ void level_emit(const LevelArgs& a, LevelSmem<WARPS>& sm, int v, bool clipped,
                                            bool fp32_decided, const double* lo, const double* hi, int depth,
                                            int given, const LaFree& lf);
 
+// One lane's box j of the chunk (j >= a.count: the lane only takes part in the
+// warp's collective child write).  All 32 lanes of the warp must call it.
+// ord_in / axis_in >= 0: this box's criterion order / split axis (SPLIT_GIVEN),
+// from a network run inline; otherwise the hint arrays (or the defaults).
 template <int FAM, int PREC, int WARPS>
 __device__ __forceinline__ void level_step(const LevelArgs& a, size_t j, LevelSmem<WARPS>& sm, unsigned& handles,
                                            int ord_in = -1, int axis_in = -1) {
