@@ -805,8 +805,8 @@ cp_status refine_graph(cp_prover* p, const cp_refine_opts& o, cp_refine_report* 
 // The lambda-independent terms of the start family travel with the boxes of
 // levels >= 1 (children) when the refinement asks for it (opts.reuse) and its
 // split can leave radii unchanged; every other refinement, and the seed level,
-// sees no aux.  A level whose aux cannot
-// be allocated goes without: its boxes recompute the terms.
+// sees no aux.  A level whose aux cannot be allocated goes without: its boxes
+// recompute the terms.
 void attach_aux(cp_prover* p, const cp_refine_opts& o) {
     // a uniform split changes every radius of every child: nothing to carry
     const bool use = o.reuse != 0 && o.family == F_START && o.policy != CP_SPLIT_UNIFORM;
